@@ -1,0 +1,332 @@
+/*
+ * vaco_av1_gpu.h -- C ABI of the B200 (sm_100a) AV1 post-decode filter library.
+ *
+ * The library replaces the scalar AV1 post-filter functions of vaco's
+ * `vaco-codec-av1` crate (paths below are relative to the vaco repository):
+ *
+ *   deblocking (AV1 spec 7.14; vaco has none, see crates/codec/vaco-codec-av1/src/lib.rs:16-18)
+ *   -> CDEF      (src/cdef.rs, driver src/decode.rs:739-896)
+ *   -> superres  (src/superres.rs:163-274, driver src/decode.rs:865-890)
+ *   -> loop restoration (src/restoration.rs:178-384, driver src/decode.rs:683-737)
+ *
+ * Conventions
+ *   - Samples are uint16_t for every bit depth, like vaco's `framebuf::Plane`
+ *     (src/framebuf.rs:16-20).  A plane is (pointer, width, height, stride);
+ *     stride is the row pitch in samples and must be >= width.
+ *   - Inputs are borrowed and never written.  Outputs are caller-allocated.
+ *   - `*_host` entry points take host pointers and are synchronous: they copy
+ *     inputs to the device, run the kernels and copy results back before
+ *     returning.  `*_dev` entry points take device pointers and only enqueue
+ *     work on `stream` (a cudaStream_t, NULL = the legacy default stream); the
+ *     status they return covers argument checks, launch errors and the data
+ *     checks, which need one small device-to-host read of a status word, so a
+ *     `*_dev` call synchronizes `stream` once before returning.
+ *   - Every entry point returns a status (vaco_av1_status) and, when `msg` is
+ *     non-NULL, stores a message id (vaco_av1_msg) naming the failed check;
+ *     vaco_av1_message() maps it to the same text vaco's
+ *     `vaco_core::Error::InvalidData(&'static str)` carries.  On any error the
+ *     output contents are unspecified, matching vaco's all-or-nothing
+ *     `Result<Plane>`.
+ *   - A context is used by one host thread at a time.  Contexts on the same
+ *     device are independent.
+ *
+ * Budget/fuel accounting (vaco-limits::Budget) stays with the caller, which
+ * allocates the outputs; see INTEGRATION.md for the Rust shim that does it.
+ */
+#ifndef VACO_AV1_GPU_H
+#define VACO_AV1_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+
+/* Mirrors the vaco_core::Error variants a filter can return
+ * (crates/core/vaco-core/src/error.rs:14-54). */
+typedef enum vaco_av1_status {
+    VACO_AV1_OK = 0,
+    VACO_AV1_INVALID_DATA = 1,   /* Error::InvalidData(msg)            */
+    VACO_AV1_UNSUPPORTED = 2,    /* Error::Unsupported(msg)            */
+    VACO_AV1_LIMIT_EXCEEDED = 3, /* Error::LimitExceeded               */
+    VACO_AV1_DEVICE_ERROR = 4,   /* CUDA runtime or launch failure     */
+    VACO_AV1_TIMEOUT = 5         /* a bounded device wait ran out      */
+} vaco_av1_status;
+
+/* Message ids.  The text of each is vaco's own error string where vaco has
+ * one (file:line of the string in crates/codec/vaco-codec-av1/). */
+typedef enum vaco_av1_msg {
+    VACO_AV1_MSG_NONE = 0,
+    VACO_AV1_MSG_CDEF_BIT_DEPTH = 1,      /* src/cdef.rs:71  */
+    VACO_AV1_MSG_CDEF_SAMPLE = 2,         /* src/cdef.rs:85  */
+    VACO_AV1_MSG_CDEF_BLOCK_PARAMS = 3,   /* src/cdef.rs:153 */
+    VACO_AV1_MSG_CDEF_STRENGTH_INDEX = 4, /* src/decode.rs:808 */
+    VACO_AV1_MSG_SR_BIT_DEPTH = 5,        /* src/superres.rs:130-132 */
+    VACO_AV1_MSG_SR_GEOMETRY = 6,         /* src/superres.rs:140 */
+    VACO_AV1_MSG_SR_SAMPLE = 7,           /* src/superres.rs:202 */
+    VACO_AV1_MSG_LR_GEOMETRY = 8,         /* src/restoration.rs:147-149 */
+    VACO_AV1_MSG_LR_UNIT_COUNT = 9,       /* src/restoration.rs:153 */
+    VACO_AV1_MSG_LR_COEFFICIENT = 10,     /* src/restoration.rs:85-87 */
+    VACO_AV1_MSG_LR_SAMPLE = 11,          /* src/restoration.rs:163-165 */
+    VACO_AV1_MSG_LR_NO_UNIT_SIZE = 12,    /* src/decode.rs:599-601 */
+    VACO_AV1_MSG_DB_PARAMS = 13,          /* deblocking (no vaco counterpart) */
+    VACO_AV1_MSG_DB_SAMPLE = 14,          /* deblocking (no vaco counterpart) */
+    VACO_AV1_MSG_FRAME_GEOMETRY = 15,     /* frame/picture descriptor mismatch */
+    VACO_AV1_MSG_NULL_ARGUMENT = 16,
+    VACO_AV1_MSG_CUDA = 17,               /* see vaco_av1_ctx_last_cuda_error() */
+    VACO_AV1_MSG_SCRATCH_LIMIT = 18,      /* request exceeds a fixed scratch size */
+    VACO_AV1_MSG_QUEUE_FULL = 19,         /* job admission refused */
+    VACO_AV1_MSG_TIMEOUT = 20,
+    VACO_AV1_MSG_COUNT = 21
+} vaco_av1_msg;
+
+/* Static, NUL-terminated text for a message id ("" for unknown ids). */
+const char* vaco_av1_message(int32_t msg);
+
+/* ---------------------------------------------------------------- context */
+
+typedef struct vaco_av1_ctx vaco_av1_ctx;
+
+/* Creates a context on CUDA device `device`.  The context owns the device
+ * scratch buffers the multi-stage entry points use and a staging area for the
+ * `*_host` entry points; both grow on demand. */
+int32_t vaco_av1_ctx_create(int32_t device, vaco_av1_ctx** out);
+void vaco_av1_ctx_destroy(vaco_av1_ctx* ctx);
+/* cudaError_t of the last VACO_AV1_DEVICE_ERROR on this context (0 if none). */
+int32_t vaco_av1_ctx_last_cuda_error(const vaco_av1_ctx* ctx);
+/* Number of kernel launches this context has issued (for launch accounting). */
+uint64_t vaco_av1_ctx_launch_count(const vaco_av1_ctx* ctx);
+
+/* ---------------------------------------------------------------- pictures */
+
+/* One reconstruction picture: vaco's `framebuf::Picture` (src/framebuf.rs:79-86).
+ * planes[1], planes[2] are NULL for a monochrome picture. */
+typedef struct vaco_av1_picture {
+    uint16_t* planes[3];
+    int32_t width[3];
+    int32_t height[3];
+    int32_t stride[3];
+} vaco_av1_picture;
+
+/* Frame geometry shared by the picture-level entry points.
+ * mi_rows/mi_cols count 4x4 luma mode-info cells; the reconstruction planes
+ * are Mi-padded (luma mi_cols*4 x mi_rows*4), as vaco allocates them
+ * (src/decode.rs:516-526). */
+typedef struct vaco_av1_frame_info {
+    int32_t bit_depth;      /* 8, 10 or 12 */
+    int32_t subsampling_x;  /* 0/1 */
+    int32_t subsampling_y;  /* 0/1 */
+    int32_t monochrome;     /* 0/1 */
+    int32_t mi_rows;
+    int32_t mi_cols;
+    int32_t coded_width;    /* visible luma width before superres */
+    int32_t coded_height;   /* visible luma height */
+    int32_t upscaled_width; /* == coded_width when superres is off */
+} vaco_av1_frame_info;
+
+/* ---------------------------------------------------------------- CDEF */
+
+/* src/cdef.rs:24-33 CdefParams (strength pairs unscaled, 8-bit units). */
+typedef struct vaco_av1_cdef_params {
+    uint8_t enabled;
+    uint8_t damping;          /* CdefDamping, 3..6 from the syntax */
+    uint8_t y_primary[8];
+    uint8_t y_secondary[8];
+    uint8_t uv_primary[8];
+    uint8_t uv_secondary[8];
+} vaco_av1_cdef_params;
+
+/* src/cdef.rs:37-54 FilterParams. */
+typedef struct vaco_av1_cdef_filter_params {
+    uint8_t width;      /* 4 or 8 */
+    uint8_t height;     /* 4 or 8 */
+    uint8_t edges;      /* left=1 right=2 top=4 bottom=8 */
+    uint8_t bit_depth;
+    uint8_t direction;  /* 0..7 */
+    uint8_t damping;
+    uint16_t primary;   /* after variance adjustment and bit-depth scaling */
+    uint16_t secondary; /* after bit-depth scaling */
+} vaco_av1_cdef_filter_params;
+
+/* cdef::find_direction (src/cdef.rs:79-124) over `n` 8x8 blocks of 64
+ * samples each: directions[i], variances[i] for block i. */
+int32_t vaco_av1_cdef_find_direction_dev(vaco_av1_ctx* ctx, void* stream,
+                                         const uint16_t* blocks, int32_t n,
+                                         int32_t bit_depth, uint8_t* directions,
+                                         uint32_t* variances, int32_t* msg);
+int32_t vaco_av1_cdef_find_direction_host(vaco_av1_ctx* ctx, const uint16_t* blocks,
+                                          int32_t n, int32_t bit_depth,
+                                          uint8_t* directions, uint32_t* variances,
+                                          int32_t* msg);
+
+/* cdef::filter_block (src/cdef.rs:142-205) over `n` 12x12 neighborhoods
+ * (144 samples each, block origin at (2,2)); outputs are 8x8 with stride 8
+ * and zeroes outside the active width x height. */
+int32_t vaco_av1_cdef_filter_block_dev(vaco_av1_ctx* ctx, void* stream,
+                                       const uint16_t* inputs,
+                                       const vaco_av1_cdef_filter_params* params,
+                                       int32_t n, uint16_t* outputs, int32_t* msg);
+int32_t vaco_av1_cdef_filter_block_host(vaco_av1_ctx* ctx, const uint16_t* inputs,
+                                        const vaco_av1_cdef_filter_params* params,
+                                        int32_t n, uint16_t* outputs, int32_t* msg);
+
+/* The frame pass of decode.rs:739-862 (apply_cdef) with its inputs explicit:
+ *   skip      mi_rows*mi_cols bytes, 1 = the 4x4 cell's skip flag (MiCell.skip)
+ *   cdef_idx  per-64x64 strength index, -1 = absent; entry (r>>4)*cdef_stride+(c>>4)
+ * `dst` receives the whole filtered picture (same extents as `src`); src and
+ * dst must not overlap.  When CDEF is disabled or every strength is zero the
+ * output is a copy of the input, as apply_cdef leaves the picture untouched. */
+int32_t vaco_av1_cdef_picture_dev(vaco_av1_ctx* ctx, void* stream,
+                                  const vaco_av1_picture* src, const vaco_av1_picture* dst,
+                                  const vaco_av1_frame_info* info, const uint8_t* skip,
+                                  const int32_t* cdef_idx, int32_t cdef_stride,
+                                  int32_t cdef_count, const vaco_av1_cdef_params* params,
+                                  int32_t* msg);
+int32_t vaco_av1_cdef_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture* src,
+                                   const vaco_av1_picture* dst,
+                                   const vaco_av1_frame_info* info, const uint8_t* skip,
+                                   const int32_t* cdef_idx, int32_t cdef_stride,
+                                   int32_t cdef_count, const vaco_av1_cdef_params* params,
+                                   int32_t* msg);
+
+/* ---------------------------------------------------------------- superres */
+
+/* superres::upscale_plane (src/superres.rs:163-216).  `input` is the Mi-padded
+ * plane (in_width x in_height); the output is output_width x height. */
+int32_t vaco_av1_superres_upscale_plane_dev(vaco_av1_ctx* ctx, void* stream,
+                                            const uint16_t* input, int32_t in_width,
+                                            int32_t in_height, int32_t in_stride,
+                                            int32_t visible_width, int32_t output_width,
+                                            int32_t height, int32_t bit_depth,
+                                            uint16_t* output, int32_t out_stride,
+                                            int32_t* msg);
+int32_t vaco_av1_superres_upscale_plane_host(vaco_av1_ctx* ctx, const uint16_t* input,
+                                             int32_t in_width, int32_t in_height,
+                                             int32_t visible_width, int32_t output_width,
+                                             int32_t height, int32_t bit_depth,
+                                             uint16_t* output, int32_t* msg);
+
+/* ---------------------------------------------------------------- restoration */
+
+enum {
+    VACO_AV1_LR_NONE = 0,
+    VACO_AV1_LR_WIENER = 1,
+    VACO_AV1_LR_SGRPROJ = 2
+};
+
+/* src/restoration.rs:48-65 RestorationUnit. */
+typedef struct vaco_av1_lr_unit {
+    int16_t type;          /* VACO_AV1_LR_* */
+    int16_t set;           /* self-guided parameter set, 0..15 */
+    int16_t vertical[3];   /* Wiener taps, outermost first */
+    int16_t horizontal[3];
+    int16_t xqd[2];        /* self-guided projection coefficients */
+} vaco_av1_lr_unit;
+
+/* src/restoration.rs:95-106 PlaneConfig. */
+typedef struct vaco_av1_lr_plane_config {
+    int32_t width;
+    int32_t height;
+    int32_t bit_depth;
+    int32_t unit_size;     /* 32, 64, 128 or 256 */
+    int32_t subsampling_y; /* 0/1 */
+} vaco_av1_lr_plane_config;
+
+/* restoration::restore_plane (src/restoration.rs:178-207).  before/after are
+ * the already-upscaled pre- and post-CDEF planes; output is width x height. */
+int32_t vaco_av1_restore_plane_dev(vaco_av1_ctx* ctx, void* stream,
+                                   const uint16_t* before, int32_t before_width,
+                                   int32_t before_height, int32_t before_stride,
+                                   const uint16_t* after, int32_t after_width,
+                                   int32_t after_height, int32_t after_stride,
+                                   const vaco_av1_lr_plane_config* config,
+                                   const vaco_av1_lr_unit* units, int32_t unit_count,
+                                   uint16_t* output, int32_t out_stride, int32_t* msg);
+int32_t vaco_av1_restore_plane_host(vaco_av1_ctx* ctx, const uint16_t* before,
+                                    int32_t before_width, int32_t before_height,
+                                    const uint16_t* after, int32_t after_width,
+                                    int32_t after_height,
+                                    const vaco_av1_lr_plane_config* config,
+                                    const vaco_av1_lr_unit* units, int32_t unit_count,
+                                    uint16_t* output, int32_t* msg);
+
+/* ---------------------------------------------------------------- deblocking */
+
+/* Frame-level loop-filter syntax kept by vaco's LoopFilterParams
+ * (src/frame_header.rs:980-983) plus loop_filter_sharpness, which vaco parses
+ * and drops (src/frame_header.rs:1013). */
+typedef struct vaco_av1_deblock_params {
+    uint8_t levels[4];  /* Y vertical, Y horizontal, U, V */
+    uint8_t sharpness;  /* 0..7 */
+    uint8_t reserved[3];
+} vaco_av1_deblock_params;
+
+/* AV1 spec 7.14 loop filter over an intra frame (vaco decodes intra frames
+ * only, src/decode.rs:511-515), in place semantics with src copied to dst:
+ *   tx_luma    mi_rows*mi_cols TX_SIZE values (AV1 TX_SIZE enum, 0..18)
+ *   tx_chroma  ((mi_rows+ssy)>>ssy)*((mi_cols+ssx)>>ssx) chroma TX_SIZE values
+ *   lvl_map    NULL for frame-uniform levels, else 4 bytes per luma Mi cell
+ *              holding the final filter level for (Y vertical, Y horizontal,
+ *              U, V) after segment and delta adjustments.
+ * The tx maps must tile each plane with transform blocks aligned to their own
+ * size, as a decoder produces them. */
+int32_t vaco_av1_deblock_picture_dev(vaco_av1_ctx* ctx, void* stream,
+                                     const vaco_av1_picture* src, const vaco_av1_picture* dst,
+                                     const vaco_av1_frame_info* info, const uint8_t* tx_luma,
+                                     const uint8_t* tx_chroma, const uint8_t* lvl_map,
+                                     const vaco_av1_deblock_params* params, int32_t* msg);
+int32_t vaco_av1_deblock_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture* src,
+                                      const vaco_av1_picture* dst,
+                                      const vaco_av1_frame_info* info, const uint8_t* tx_luma,
+                                      const uint8_t* tx_chroma, const uint8_t* lvl_map,
+                                      const vaco_av1_deblock_params* params, int32_t* msg);
+
+/* ---------------------------------------------------------------- whole chain */
+
+/* Frame-level restoration mode, src/restoration.rs:17-27 RestorationType. */
+enum {
+    VACO_AV1_FRAME_LR_NONE = 0,
+    VACO_AV1_FRAME_LR_SWITCHABLE = 1,
+    VACO_AV1_FRAME_LR_WIENER = 2,
+    VACO_AV1_FRAME_LR_SGRPROJ = 3
+};
+
+/* Everything decode_frame (src/decode.rs:553-559) hands the post-filters,
+ * with deblocking in front.  Pointers are device pointers for the `_dev`
+ * entry points and host pointers for the `_host` ones. */
+typedef struct vaco_av1_frame_job {
+    vaco_av1_frame_info info;
+    vaco_av1_picture src;            /* reconstruction, Mi-padded */
+    vaco_av1_picture dst;            /* visible output: upscaled_width x coded_height */
+    const uint8_t* tx_luma;
+    const uint8_t* tx_chroma;
+    const uint8_t* lvl_map;          /* may be NULL */
+    const uint8_t* skip;
+    const int32_t* cdef_idx;
+    int32_t cdef_stride;
+    int32_t cdef_count;
+    vaco_av1_deblock_params deblock;
+    vaco_av1_cdef_params cdef;
+    int32_t lr_type[3];              /* VACO_AV1_FRAME_LR_* per plane */
+    int32_t lr_unit_size[3];
+    const vaco_av1_lr_unit* lr_units[3];
+    int32_t lr_unit_count[3];
+} vaco_av1_frame_job;
+
+/* deblock -> CDEF -> superres (when upscaled_width != coded_width) -> loop
+ * restoration for one frame.  The output is the picture vaco's decode_frame
+ * would hand to pic_to_frame, cropped to the visible size; subsampled frames
+ * need even coded/upscaled widths and heights. */
+int32_t vaco_av1_postfilter_frame_dev(vaco_av1_ctx* ctx, void* stream,
+                                      const vaco_av1_frame_job* job, int32_t* msg);
+int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job,
+                                       int32_t* msg);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* VACO_AV1_GPU_H */
