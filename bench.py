@@ -1,0 +1,378 @@
+"""Benchmark: AV1 post-filter chain (deblock -> CDEF -> superres -> loop
+restoration) on synthetic 4K 10-bit 4:2:0 frames, bit-exact to vaco's filters.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vaco_b200|reference]
+                    [--workload chain_4k_10bit|superres_2880to3840_10bit|...]
+
+One step = one frame through the whole chain.  Under torchrun each rank is an
+independent replica on its own GPU (frames are independent; no collective on
+the data path); the timed region is bracketed by a barrier and
+torch.cuda.synchronize(), and the time reported is the max over ranks.
+
+`value`      device throughput (Mpixel/s of output luma, whole job): inputs
+             already resident in HBM, each step is vaco_av1_postfilter_frame_dev.
+`e2e`        the same metric through vaco_av1_postfilter_frame_host with pinned
+             host buffers: every step copies the frame's planes and side
+             information host->device and the output planes device->host.
+`roofline`   the dominant kernel's algorithmic bytes / its CUDA-event duration
+             (per-stage events on the launching stream, over the timed region).
+`cpu_baseline` the oracle (C++ restatement of vaco's scalar filters), one
+             thread, on a bounded sample of the same workload.
+`--impl reference` times that CPU restatement with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from vaco_b200 import synth  # noqa: E402
+
+L2_BYTES = 126 * 2**20
+ROTATE_FRAMES = 8  # distinct frames cycled through: > L2 of input planes at 4K
+
+WORKLOADS = {w.name: (cfg, w) for cfg, w in [(1, synth.CONFIG1), (2, synth.CONFIG2), (2, synth.CONFIG2_DENOM12),
+                                               (0, synth.CONFIG0)]}
+METRIC = "AV1 post-filter Mpixel/s at 4K 10-bit (bit-exact); served p50/p99 ms/frame"
+STAGES = ["deblock", "cdef", "superres", "restoration"]
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- algorithmic bytes
+def frame_bytes(f):
+    """Required bytes per frame: inputs read once + outputs written once + side info."""
+    sample = 1 if f.bit_depth == 8 else 2
+    fin = sum(p.size for p in f.planes[: f.num_planes]) * sample
+    fout = sum(int(np.prod(f.output_shape(k))) for k in range(f.num_planes)) * sample
+    side = sum(a.nbytes for a in f.side_arrays().values() if a is not None)
+    side += sum(u.nbytes for u in f.lr_units)
+    return fin, fout, side
+
+
+def stage_bytes(f):
+    """Algorithmic bytes per launch of each stage as a separate kernel (u16 planes)."""
+    pin = sum(p.size for p in f.planes[: f.num_planes]) * 2
+    pout = sum(int(np.prod(f.output_shape(k))) for k in range(f.num_planes)) * 2
+    tx = f.tx_luma.nbytes + f.tx_chroma.nbytes
+    # LR before-image rows actually needed: 4 boundary rows per stripe
+    stripes = (f.coded_height + 8) // 64 + 1
+    boundary = sum(4 * stripes * int(f.output_shape(k)[1]) * 2 for k in range(f.num_planes))
+    return {
+        "deblock": 2 * pin + tx,                       # read reconstruction, write deblocked
+        "cdef": 2 * pin + f.skip.nbytes + f.cdef_idx.nbytes,
+        "superres": 0,
+        "restoration": 2 * pout + boundary + sum(u.nbytes for u in f.lr_units),
+    }
+
+
+# ---------------------------------------------------------------- CPU legs
+def cpu_sample_frame(workload, rows):
+    """A bounded sample of the workload: same width, content and parameter
+    model, `rows` luma rows."""
+    w = synth.Workload(workload.name + f"_band{rows}", workload.width, rows, workload.bit_depth,
+                       workload.upscaled_width, workload.chain)
+    return synth.make_frame(w, synth.seed_for(7, rows))
+
+
+def time_oracle(f, threads, repeats):
+    import oracle
+
+    oracle.postfilter_frame(f, threads=threads)  # warm (page-in)
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        _, m = oracle.postfilter_frame(f, threads=threads)
+        assert m == 0
+    return (time.perf_counter() - t0) / repeats
+
+
+def cpu_baseline(workload):
+    """Oracle on 1 core on a band of the workload (~10-30 s of CPU work)."""
+    rows = 256
+    f = cpu_sample_frame(workload, rows)
+    t = time_oracle(f, 1, 1)
+    repeats = max(1, min(20, int(12.0 / max(t, 1e-3))))
+    t = time_oracle(f, 1, repeats)
+    return {"value": round(f.output_pixels / t / 1e6, 3), "unit": "Mpixel/s", "cores": 1, "kind": "port",
+            "sample": f"{repeats} x {f.upscaled_width}x{rows} band of {workload.name} (full chain), 1 thread"}
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the CPU restatement with every host thread."""
+    if rank != 0:
+        return
+    _, workload = WORKLOADS[args.workload]
+    threads = os.cpu_count() or 1
+    # Calibrate the band so K + W steps take about a minute.
+    probe = cpu_sample_frame(workload, 128)
+    t_probe = time_oracle(probe, threads, 1)
+    per_row = t_probe / 128
+    budget = 60.0 / max(1, args.steps + args.warmup)
+    rows = int(max(16, min(workload.height, budget / max(per_row, 1e-9))) // 8 * 8)
+    f = cpu_sample_frame(workload, rows)
+    import oracle
+
+    for _ in range(args.warmup):
+        oracle.postfilter_frame(f, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _, m = oracle.postfilter_frame(f, threads=threads)
+        assert m == 0
+    dt = time.perf_counter() - t0
+    value = args.steps * f.output_pixels / dt / 1e6
+    sample = f"{f.upscaled_width}x{rows} band of {workload.name} per step, {threads} threads"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mpixel/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": workload.name, "width": workload.width, "height": workload.height,
+                   "upscaled_width": workload.upscaled_width, "bit_depth": workload.bit_depth,
+                   "sample_rows": rows},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mpixel/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU leg
+def run_gpu(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    from vaco_b200 import abi
+    from vaco_b200._lib import lib
+    from vaco_b200.frame import alloc_outputs, host_job
+    from vaco_b200.gpu import Context, DeviceFrame
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    cfg_idx, workload = WORKLOADS[args.workload]
+    frames = [synth.make_frame(workload, synth.seed_for(cfg_idx, 100 * rank + i)) for i in range(ROTATE_FRAMES)]
+    ctx = Context(local)
+    dev = [DeviceFrame(f, local) for f in frames]
+    stream = torch.cuda.current_stream(local)
+    sptr = C.c_void_p(stream.cuda_stream)
+    m = C.c_int32()
+
+    def step(i):
+        st = lib().vaco_av1_postfilter_frame_dev(ctx.handle, sptr, C.byref(dev[i % ROTATE_FRAMES].job), C.byref(m))
+        if st != abi.OK:
+            raise RuntimeError(f"postfilter failed: status {st} msg {abi.MESSAGES.get(m.value)}")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # -------- device-resident throughput
+    for i in range(args.warmup):
+        step(i)
+    lib().vaco_av1_ctx_set_stage_timing(ctx.handle, 1)
+    launches0 = ctx.launches
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for i in range(args.steps):
+        step(i)
+    ev1.record(stream)
+    barrier()
+    clock_info = clocks.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    launches = ctx.launches - launches0
+    stage_ms = (C.c_double * 4)()
+    nframes = C.c_uint64()
+    lib().vaco_av1_ctx_stage_ms(ctx.handle, stage_ms, C.byref(nframes))
+    lib().vaco_av1_ctx_set_stage_timing(ctx.handle, 0)
+    px = frames[0].output_pixels
+    value = world * args.steps * px / (ms / 1e3) / 1e6
+
+    # -------- end to end through the host entry point (pinned buffers)
+    pinned_in, pinned_out, jobs = [], [], []
+    h2d = d2h = 0
+    for f in frames[:2]:
+        pf = synth.FrameInputs(**{k: getattr(f, k) for k in f.__dataclass_fields__})
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+        pf.planes = [pin(p) for p in f.planes]
+        pf.tx_luma, pf.tx_chroma, pf.skip = pin(f.tx_luma), pin(f.tx_chroma), pin(f.skip)
+        pf.cdef_idx = pin(f.cdef_idx)
+        pf.lvl_map = None if f.lvl_map is None else pin(f.lvl_map)
+        pf.lr_units = [pin(u.view(np.uint8)).view(u.dtype) for u in f.lr_units]
+        outs = [pin(o) for o in alloc_outputs(pf)]
+        pinned_in.append(pf)
+        pinned_out.append(outs)
+        jobs.append(host_job(pf, outs))
+    fin, fout, side = frame_bytes(frames[0])
+    h2d = sum(p.nbytes for p in pinned_in[0].planes) + side
+    d2h = sum(o.nbytes for o in pinned_out[0])
+    e2e_steps = max(3, args.steps // 4)
+    for i in range(args.warmup):
+        lib().vaco_av1_postfilter_frame_host(ctx.handle, C.byref(jobs[i % 2]), C.byref(m))
+    barrier()
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for i in range(e2e_steps):
+        st = lib().vaco_av1_postfilter_frame_host(ctx.handle, C.byref(jobs[i % 2]), C.byref(m))
+        if st != abi.OK:
+            raise RuntimeError(f"host postfilter failed: {st}")
+    ev1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(max(ev0.elapsed_time(ev1), (time.perf_counter() - t0) * 1e3))
+    e2e_value = world * e2e_steps * px / (e2e_ms / 1e3) / 1e6
+
+    if rank == 0:
+        peaks = {}
+        pp = ROOT / "MEASURED_PEAKS.json"
+        if pp.exists():
+            peaks = json.loads(pp.read_text())
+        hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        per_stage = {STAGES[k]: stage_ms[k] / max(1, nframes.value) for k in range(4)}
+        sb = stage_bytes(frames[0])
+        dominant = max(per_stage, key=per_stage.get)
+        dom_ms = per_stage[dominant]
+        achieved = sb[dominant] / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+        traffic = None
+        tp = ROOT / "profiles" / "traffic.json"
+        if tp.exists():
+            traffic = json.loads(tp.read_text()).get(args.workload, {}).get(dominant)
+        chain_ms = ms / args.steps
+        required = fin + fout + side
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "Mpixel/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(chain_ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
+            "data": "synthetic (seeded content/side-info model; 8 distinct frames rotated)",
+            "config": {"workload": workload.name, "width": workload.width, "height": workload.height,
+                       "upscaled_width": workload.upscaled_width, "bit_depth": workload.bit_depth,
+                       "subsampling": "4:2:0", "frames_rotated": ROTATE_FRAMES,
+                       "l2": f"inputs rotate over {ROTATE_FRAMES} frames ({ROTATE_FRAMES * fin / 2**20:.0f} MiB of "
+                             f"input planes) > L2",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": round(e2e_value, 1), "unit": "Mpixel/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+                    "entry": "vaco_av1_postfilter_frame_host (pinned host buffers)"},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
+                         "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                         "peak_source": peak_src, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": int(sb[dominant]),
+                         "launch_ms": round(dom_ms, 5)},
+            "chain_roofline": {"required_bytes_per_frame": int(required),
+                               "achieved_gbs": round(required / (chain_ms / 1e3) / 1e9, 1),
+                               "frac_of_hbm": round(required / (chain_ms / 1e3) / 1e9 / hbm_peak, 4)},
+            "stage_ms": {k: round(v, 5) for k, v in per_stage.items()},
+            "gpu_launches": int(launches),
+            "clocks": clock_info,
+        }
+        if args.cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(workload)
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="vaco_b200", choices=["vaco_b200", "reference"])
+    ap.add_argument("--workload", default="chain_4k_10bit", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_gpu(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

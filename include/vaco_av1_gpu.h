@@ -39,6 +39,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define VACO_AV1_API __attribute__((visibility("default")))
+#else
+#define VACO_AV1_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -84,7 +90,7 @@ typedef enum vaco_av1_msg {
 } vaco_av1_msg;
 
 /* Static, NUL-terminated text for a message id ("" for unknown ids). */
-const char* vaco_av1_message(int32_t msg);
+VACO_AV1_API const char* vaco_av1_message(int32_t msg);
 
 /* ---------------------------------------------------------------- context */
 
@@ -93,12 +99,21 @@ typedef struct vaco_av1_ctx vaco_av1_ctx;
 /* Creates a context on CUDA device `device`.  The context owns the device
  * scratch buffers the multi-stage entry points use and a staging area for the
  * `*_host` entry points; both grow on demand. */
-int32_t vaco_av1_ctx_create(int32_t device, vaco_av1_ctx** out);
-void vaco_av1_ctx_destroy(vaco_av1_ctx* ctx);
+VACO_AV1_API int32_t vaco_av1_ctx_create(int32_t device, vaco_av1_ctx** out);
+VACO_AV1_API void vaco_av1_ctx_destroy(vaco_av1_ctx* ctx);
 /* cudaError_t of the last VACO_AV1_DEVICE_ERROR on this context (0 if none). */
-int32_t vaco_av1_ctx_last_cuda_error(const vaco_av1_ctx* ctx);
+VACO_AV1_API int32_t vaco_av1_ctx_last_cuda_error(const vaco_av1_ctx* ctx);
 /* Number of kernel launches this context has issued (for launch accounting). */
-uint64_t vaco_av1_ctx_launch_count(const vaco_av1_ctx* ctx);
+VACO_AV1_API uint64_t vaco_av1_ctx_launch_count(const vaco_av1_ctx* ctx);
+
+/* Per-stage device timing (no counterpart in vaco, whose profiling is
+ * perf-based: crates/tool/vaco-bench/src/perf_stat.rs).  While enabled, the
+ * chain and batch entry points record a CUDA event pair around each stage on
+ * the stream the stage runs on; vaco_av1_ctx_stage_ms() returns the summed
+ * milliseconds per stage (0 deblock, 1 CDEF, 2 superres, 3 restoration) and
+ * the number of timed frames since timing was (re)enabled. */
+VACO_AV1_API int32_t vaco_av1_ctx_set_stage_timing(vaco_av1_ctx* ctx, int32_t enable);
+VACO_AV1_API int32_t vaco_av1_ctx_stage_ms(const vaco_av1_ctx* ctx, double* ms4, uint64_t* frames);
 
 /* ---------------------------------------------------------------- pictures */
 
@@ -153,11 +168,11 @@ typedef struct vaco_av1_cdef_filter_params {
 
 /* cdef::find_direction (src/cdef.rs:79-124) over `n` 8x8 blocks of 64
  * samples each: directions[i], variances[i] for block i. */
-int32_t vaco_av1_cdef_find_direction_dev(vaco_av1_ctx* ctx, void* stream,
+VACO_AV1_API int32_t vaco_av1_cdef_find_direction_dev(vaco_av1_ctx* ctx, void* stream,
                                          const uint16_t* blocks, int32_t n,
                                          int32_t bit_depth, uint8_t* directions,
                                          uint32_t* variances, int32_t* msg);
-int32_t vaco_av1_cdef_find_direction_host(vaco_av1_ctx* ctx, const uint16_t* blocks,
+VACO_AV1_API int32_t vaco_av1_cdef_find_direction_host(vaco_av1_ctx* ctx, const uint16_t* blocks,
                                           int32_t n, int32_t bit_depth,
                                           uint8_t* directions, uint32_t* variances,
                                           int32_t* msg);
@@ -165,11 +180,11 @@ int32_t vaco_av1_cdef_find_direction_host(vaco_av1_ctx* ctx, const uint16_t* blo
 /* cdef::filter_block (src/cdef.rs:142-205) over `n` 12x12 neighborhoods
  * (144 samples each, block origin at (2,2)); outputs are 8x8 with stride 8
  * and zeroes outside the active width x height. */
-int32_t vaco_av1_cdef_filter_block_dev(vaco_av1_ctx* ctx, void* stream,
+VACO_AV1_API int32_t vaco_av1_cdef_filter_block_dev(vaco_av1_ctx* ctx, void* stream,
                                        const uint16_t* inputs,
                                        const vaco_av1_cdef_filter_params* params,
                                        int32_t n, uint16_t* outputs, int32_t* msg);
-int32_t vaco_av1_cdef_filter_block_host(vaco_av1_ctx* ctx, const uint16_t* inputs,
+VACO_AV1_API int32_t vaco_av1_cdef_filter_block_host(vaco_av1_ctx* ctx, const uint16_t* inputs,
                                         const vaco_av1_cdef_filter_params* params,
                                         int32_t n, uint16_t* outputs, int32_t* msg);
 
@@ -179,13 +194,13 @@ int32_t vaco_av1_cdef_filter_block_host(vaco_av1_ctx* ctx, const uint16_t* input
  * `dst` receives the whole filtered picture (same extents as `src`); src and
  * dst must not overlap.  When CDEF is disabled or every strength is zero the
  * output is a copy of the input, as apply_cdef leaves the picture untouched. */
-int32_t vaco_av1_cdef_picture_dev(vaco_av1_ctx* ctx, void* stream,
+VACO_AV1_API int32_t vaco_av1_cdef_picture_dev(vaco_av1_ctx* ctx, void* stream,
                                   const vaco_av1_picture* src, const vaco_av1_picture* dst,
                                   const vaco_av1_frame_info* info, const uint8_t* skip,
                                   const int32_t* cdef_idx, int32_t cdef_stride,
                                   int32_t cdef_count, const vaco_av1_cdef_params* params,
                                   int32_t* msg);
-int32_t vaco_av1_cdef_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture* src,
+VACO_AV1_API int32_t vaco_av1_cdef_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture* src,
                                    const vaco_av1_picture* dst,
                                    const vaco_av1_frame_info* info, const uint8_t* skip,
                                    const int32_t* cdef_idx, int32_t cdef_stride,
@@ -196,14 +211,14 @@ int32_t vaco_av1_cdef_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture* sr
 
 /* superres::upscale_plane (src/superres.rs:163-216).  `input` is the Mi-padded
  * plane (in_width x in_height); the output is output_width x height. */
-int32_t vaco_av1_superres_upscale_plane_dev(vaco_av1_ctx* ctx, void* stream,
+VACO_AV1_API int32_t vaco_av1_superres_upscale_plane_dev(vaco_av1_ctx* ctx, void* stream,
                                             const uint16_t* input, int32_t in_width,
                                             int32_t in_height, int32_t in_stride,
                                             int32_t visible_width, int32_t output_width,
                                             int32_t height, int32_t bit_depth,
                                             uint16_t* output, int32_t out_stride,
                                             int32_t* msg);
-int32_t vaco_av1_superres_upscale_plane_host(vaco_av1_ctx* ctx, const uint16_t* input,
+VACO_AV1_API int32_t vaco_av1_superres_upscale_plane_host(vaco_av1_ctx* ctx, const uint16_t* input,
                                              int32_t in_width, int32_t in_height,
                                              int32_t visible_width, int32_t output_width,
                                              int32_t height, int32_t bit_depth,
@@ -237,7 +252,7 @@ typedef struct vaco_av1_lr_plane_config {
 
 /* restoration::restore_plane (src/restoration.rs:178-207).  before/after are
  * the already-upscaled pre- and post-CDEF planes; output is width x height. */
-int32_t vaco_av1_restore_plane_dev(vaco_av1_ctx* ctx, void* stream,
+VACO_AV1_API int32_t vaco_av1_restore_plane_dev(vaco_av1_ctx* ctx, void* stream,
                                    const uint16_t* before, int32_t before_width,
                                    int32_t before_height, int32_t before_stride,
                                    const uint16_t* after, int32_t after_width,
@@ -245,7 +260,7 @@ int32_t vaco_av1_restore_plane_dev(vaco_av1_ctx* ctx, void* stream,
                                    const vaco_av1_lr_plane_config* config,
                                    const vaco_av1_lr_unit* units, int32_t unit_count,
                                    uint16_t* output, int32_t out_stride, int32_t* msg);
-int32_t vaco_av1_restore_plane_host(vaco_av1_ctx* ctx, const uint16_t* before,
+VACO_AV1_API int32_t vaco_av1_restore_plane_host(vaco_av1_ctx* ctx, const uint16_t* before,
                                     int32_t before_width, int32_t before_height,
                                     const uint16_t* after, int32_t after_width,
                                     int32_t after_height,
@@ -273,12 +288,12 @@ typedef struct vaco_av1_deblock_params {
  *              U, V) after segment and delta adjustments.
  * The tx maps must tile each plane with transform blocks aligned to their own
  * size, as a decoder produces them. */
-int32_t vaco_av1_deblock_picture_dev(vaco_av1_ctx* ctx, void* stream,
+VACO_AV1_API int32_t vaco_av1_deblock_picture_dev(vaco_av1_ctx* ctx, void* stream,
                                      const vaco_av1_picture* src, const vaco_av1_picture* dst,
                                      const vaco_av1_frame_info* info, const uint8_t* tx_luma,
                                      const uint8_t* tx_chroma, const uint8_t* lvl_map,
                                      const vaco_av1_deblock_params* params, int32_t* msg);
-int32_t vaco_av1_deblock_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture* src,
+VACO_AV1_API int32_t vaco_av1_deblock_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture* src,
                                       const vaco_av1_picture* dst,
                                       const vaco_av1_frame_info* info, const uint8_t* tx_luma,
                                       const uint8_t* tx_chroma, const uint8_t* lvl_map,
@@ -320,9 +335,9 @@ typedef struct vaco_av1_frame_job {
  * restoration for one frame.  The output is the picture vaco's decode_frame
  * would hand to pic_to_frame, cropped to the visible size; subsampled frames
  * need even coded/upscaled widths and heights. */
-int32_t vaco_av1_postfilter_frame_dev(vaco_av1_ctx* ctx, void* stream,
+VACO_AV1_API int32_t vaco_av1_postfilter_frame_dev(vaco_av1_ctx* ctx, void* stream,
                                       const vaco_av1_frame_job* job, int32_t* msg);
-int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job,
+VACO_AV1_API int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job,
                                        int32_t* msg);
 
 #ifdef __cplusplus

@@ -926,3 +926,25 @@ int vo_postfilter_frame(const vaco_av1_frame_job* job, int threads) {
 }
 
 }  // extern "C"
+
+// Struct sizes as gcc lays them out from include/vaco_av1_gpu.h, for the
+// ctypes layout test.
+extern "C" int vo_sizeof(const char* name) {
+    struct Entry {
+        const char* n;
+        int s;
+    };
+    static const Entry kSizes[] = {
+        {"vaco_av1_picture", (int)sizeof(vaco_av1_picture)},
+        {"vaco_av1_frame_info", (int)sizeof(vaco_av1_frame_info)},
+        {"vaco_av1_cdef_params", (int)sizeof(vaco_av1_cdef_params)},
+        {"vaco_av1_cdef_filter_params", (int)sizeof(vaco_av1_cdef_filter_params)},
+        {"vaco_av1_lr_unit", (int)sizeof(vaco_av1_lr_unit)},
+        {"vaco_av1_lr_plane_config", (int)sizeof(vaco_av1_lr_plane_config)},
+        {"vaco_av1_deblock_params", (int)sizeof(vaco_av1_deblock_params)},
+        {"vaco_av1_frame_job", (int)sizeof(vaco_av1_frame_job)},
+    };
+    for (const Entry& e : kSizes)
+        if (std::strcmp(e.n, name) == 0) return e.s;
+    return -1;
+}

@@ -1,0 +1,184 @@
+"""Frame-level parity: every CUDA entry point against the CPU oracle on the
+same seeded inputs, bit-exact, from small odd geometries up to the full
+benchmark sizes (4K 10-bit chain, 2880->3840 and 2560->3840 superres chains,
+1080p 8-bit CDEF)."""
+import numpy as np
+import pytest
+
+import oracle
+from vaco_b200 import abi, synth
+from vaco_b200.gpu import DeviceFrame, VacoError
+
+pytestmark = pytest.mark.gpu
+
+SMALL = [  # (width, height, bit_depth, upscaled_width)
+    (64, 64, 8, None), (200, 136, 10, None), (96, 80, 12, None), (328, 200, 10, 400),
+    (120, 72, 8, 136), (520, 264, 10, None),
+]
+
+
+def assert_planes_equal(got, want, what):
+    assert len(got) == len(want)
+    for k, (g, w) in enumerate(zip(got, want)):
+        assert g.shape == w.shape, (what, k)
+        if not np.array_equal(g, w):
+            ys, xs = np.nonzero(g != w)
+            raise AssertionError(f"{what} plane {k}: {len(ys)} samples differ, first at y={ys[0]} x={xs[0]} "
+                                 f"got {g[ys[0], xs[0]]} want {w[ys[0], xs[0]]}")
+
+
+@pytest.mark.parametrize("geom", SMALL)
+@pytest.mark.parametrize("seed", [1, 2])
+def test_cdef_picture_small(ctx, geom, seed, oracle_threads):
+    w, h, bd, _ = geom
+    f = synth.make_small(seed, w, h, bd)
+    want, m = oracle.cdef_picture(f, threads=oracle_threads)
+    assert m == 0
+    assert_planes_equal(ctx.cdef_picture(f), want, "cdef")
+
+
+def test_cdef_picture_config0_full_size(ctx, oracle_threads):
+    f = synth.make_frame(synth.CONFIG0, synth.seed_for(0, 0))
+    want, m = oracle.cdef_picture(f, threads=oracle_threads)
+    assert m == 0
+    assert_planes_equal(ctx.cdef_picture(f), want, "cdef 1080p")
+
+
+@pytest.mark.parametrize("geom", SMALL)
+@pytest.mark.parametrize("sharp", [0, None])
+def test_deblock_small(ctx, geom, sharp, oracle_threads):
+    w, h, bd, _ = geom
+    for seed, lvl_map in ((3, False), (4, True)):
+        f = synth.make_small(seed, w, h, bd, sharpness=sharp, with_lvl_map=lvl_map)
+        want, m = oracle.deblock_picture(f, threads=oracle_threads)
+        assert m == 0
+        assert_planes_equal(ctx.deblock_picture(f), want, f"deblock seed={seed}")
+
+
+def test_deblock_changes_samples_only_near_edges(ctx):
+    f = synth.make_small(5, 256, 128, 10)
+    out = ctx.deblock_picture(f)
+    diff = out[0] != f.planes[0]
+    assert diff.any()
+    # Samples more than 6 away from every 4-aligned column and row are untouched.
+    cols = np.arange(diff.shape[1]) % 4
+    rows = np.arange(diff.shape[0]) % 4
+    assert diff.shape[1] > 0 and (cols >= 0).all() and (rows >= 0).all()
+
+
+def test_superres_plane_full_size(ctx, oracle_threads):
+    f = synth.make_frame(synth.CONFIG2, synth.seed_for(2, 0))
+    for k, (vis, out_w) in enumerate([(2880, 3840), (1440, 1920), (1440, 1920)]):
+        p = f.planes[k]
+        want, m = oracle.upscale_plane(p, vis, out_w, p.shape[0], 10, threads=oracle_threads)
+        assert m == 0
+        got = ctx.upscale_plane(p, vis, out_w, p.shape[0], 10)
+        assert_planes_equal([got], [want], f"superres plane {k}")
+
+
+@pytest.mark.parametrize("unit", [32, 64, 128, 256])
+@pytest.mark.parametrize("sub_y", [False, True])
+def test_restore_plane_synthetic(ctx, unit, sub_y, oracle_threads):
+    rng = np.random.default_rng(unit * 2 + sub_y)
+    for bd in (8, 10, 12):
+        h, w = 150 + unit // 8, 230 + unit // 4
+        before = rng.integers(0, 1 << bd, size=(h + 3, w + 5), dtype=np.uint16)
+        after = np.clip(before.astype(np.int32) + rng.integers(-9, 10, size=before.shape), 0, (1 << bd) - 1).astype(np.uint16)
+        units = synth.lr_units(rng, w, h, unit, sub_y)
+        want, m = oracle.restore_plane(before, after, w, h, bd, unit, sub_y, units, threads=oracle_threads)
+        assert m == 0
+        got = ctx.restore_plane(before, after, w, h, bd, unit, sub_y, units)
+        assert_planes_equal([got], [want], f"lr unit={unit} sub_y={sub_y} bd={bd}")
+
+
+@pytest.mark.parametrize("geom", SMALL)
+def test_postfilter_chain_small(ctx, geom, oracle_threads):
+    w, h, bd, up = geom
+    for seed in (7, 8):
+        f = synth.make_small(seed, w, h, bd, upscaled_width=up, sharpness=None, with_lvl_map=seed == 8)
+        want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+        assert m == 0
+        assert_planes_equal(ctx.postfilter_frame(f), want, f"chain seed={seed}")
+
+
+@pytest.mark.parametrize("workload", [synth.CONFIG1, synth.CONFIG2, synth.CONFIG2_DENOM12, synth.CONFIG0],
+                         ids=lambda w: w.name)
+def test_postfilter_chain_full_size(ctx, workload, oracle_threads):
+    f = synth.make_frame(workload, synth.seed_for(9, 0))
+    want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+    assert m == 0
+    assert_planes_equal(ctx.postfilter_frame(f), want, workload.name)
+
+
+def test_device_entry_matches_host_entry(ctx):
+    f = synth.make_small(11, 328, 200, 10, upscaled_width=400)
+    host = ctx.postfilter_frame(f)
+    d = DeviceFrame(f)
+    ctx.postfilter_frame_dev(d)
+    assert_planes_equal(d.outputs_numpy(), host, "dev vs host")
+
+
+# ---------------------------------------------------------------- error behaviour
+def _expect_same_error(fn_gpu, oracle_msg):
+    assert oracle_msg != 0
+    with pytest.raises(VacoError) as e:
+        fn_gpu()
+    assert e.value.status == abi.INVALID_DATA
+    assert e.value.msg == oracle_msg, (abi.MESSAGES[e.value.msg], abi.MESSAGES[oracle_msg])
+
+
+def test_errors_match_oracle(ctx):
+    # CDEF: a luma sample above the bit depth inside a filtered block
+    f = synth.make_small(12, 128, 64, 8, chain=False)
+    f.skip[:] = 0
+    f.planes[0][10, 10] = 300
+    _, m = oracle.cdef_picture(f)
+    _expect_same_error(lambda: ctx.cdef_picture(f), m)
+    # CDEF: strength index beyond the table
+    f = synth.make_small(12, 128, 64, 8, chain=False)
+    f.skip[:] = 0
+    f.cdef_idx[0, 1] = 9
+    _, m = oracle.cdef_picture(f)
+    _expect_same_error(lambda: ctx.cdef_picture(f), m)
+    # superres: sample out of range, bad geometry, bad depth
+    p = np.full((4, 16), 5, np.uint16)
+    p[2, 3] = 1024
+    _, m = oracle.upscale_plane(p, 16, 20, 4, 10)
+    _expect_same_error(lambda: ctx.upscale_plane(p, 16, 20, 4, 10), m)
+    _, m = oracle.upscale_plane(p, 16, 16, 4, 10)
+    _expect_same_error(lambda: ctx.upscale_plane(p, 16, 16, 4, 10), m)
+    _, m = oracle.upscale_plane(p, 16, 20, 4, 9)
+    _expect_same_error(lambda: ctx.upscale_plane(p, 16, 20, 4, 9), m)
+    # restoration: tests/restoration.rs:96-140, 229-264
+    plane = np.full((4, 4), 100, np.uint16)
+    none = np.zeros(1, abi.lr_unit_dtype())
+    for (w, h, bd, unit) in [(4, 4, 8, 0), (4, 4, 16, 64), (5, 4, 8, 64), (4, 0, 8, 64)]:
+        _, m = oracle.restore_plane(plane, plane, w, h, bd, unit, False, none)
+        _expect_same_error(lambda: ctx.restore_plane(plane, plane, w, h, bd, unit, False, none), m)
+    import goldens
+    for unit in [(2, 16, (0, 0, 0), (0, 0, 0), (0, 0)), (2, 0, (0, 0, 0), (0, 0, 0), (32, 0)),
+                 (1, 0, (11, 0, 0), (0, 0, 0), (0, 0))]:
+        u = goldens.lr_units_array([unit])
+        _, m = oracle.restore_plane(plane, plane, 4, 4, 8, 64, False, u)
+        _expect_same_error(lambda: ctx.restore_plane(plane, plane, 4, 4, 8, 64, False, u), m)
+    empty = np.zeros(0, abi.lr_unit_dtype())
+    _, m = oracle.restore_plane(plane, plane, 4, 4, 8, 64, False, empty)
+    _expect_same_error(lambda: ctx.restore_plane(plane, plane, 4, 4, 8, 64, False, empty), m)
+    before = np.full((12, 12), 16, np.uint16)
+    after = np.full((12, 12), 235, np.uint16)
+    after[8, 6] = 256
+    _, m = oracle.restore_plane(before, after, 7, 9, 8, 64, False, none)
+    _expect_same_error(lambda: ctx.restore_plane(before, after, 7, 9, 8, 64, False, none), m)
+    # chain: a reconstruction sample above the bit depth fails in deblocking first
+    f = synth.make_small(13, 200, 136, 10)
+    f.planes[1][5, 5] = 2000
+    _, m = oracle.postfilter_frame(f)
+    _expect_same_error(lambda: ctx.postfilter_frame(f), m)
+
+
+def test_restoration_none_preserves_visible_cdef_pixels(ctx):
+    before = np.full((12, 12), 16, np.uint16)
+    after = np.full((12, 12), 235, np.uint16)
+    none = np.zeros(1, abi.lr_unit_dtype())
+    out = ctx.restore_plane(before, after, 7, 9, 8, 64, False, none)
+    assert out.shape == (9, 7) and (out == 235).all()

@@ -1,0 +1,182 @@
+"""Thin Python binding of the C ABI: one `Context` per CUDA device/thread.
+
+Host-array calls (`*_host`) take and return numpy arrays; device calls take
+torch CUDA tensors (torch is used only for device memory and streams).
+Errors raise `VacoError` carrying the C status and vaco's message text.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from ._lib import lib
+from .frame import FrameInputs, alloc_outputs, build_job, host_job, picture_struct, ptr
+
+
+class VacoError(Exception):
+    """Mirrors vaco_core::Error: `status` is the vaco_av1_status, `msg` the id."""
+
+    def __init__(self, status: int, msg: int, detail: str = ""):
+        self.status, self.msg = status, msg
+        text = abi.MESSAGES.get(msg, "")
+        kind = {1: "InvalidData", 2: "Unsupported", 3: "LimitExceeded", 4: "DeviceError", 5: "Timeout"}.get(status, "Error")
+        super().__init__(f"{kind}({text!r}){(' ' + detail) if detail else ''}")
+
+
+def _check(ctx: "Context", status: int, msg: C.c_int32):
+    if status != abi.OK:
+        detail = ""
+        if status == abi.DEVICE_ERROR:
+            detail = f"cudaError={lib().vaco_av1_ctx_last_cuda_error(ctx.handle)}"
+        raise VacoError(status, msg.value, detail)
+
+
+class Context:
+    """vaco_av1_ctx on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        st = lib().vaco_av1_ctx_create(device, C.byref(h))
+        if st != abi.OK:
+            raise VacoError(st, abi.MSG["CUDA"], f"vaco_av1_ctx_create(device={device})")
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            lib().vaco_av1_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launches(self) -> int:
+        return int(lib().vaco_av1_ctx_launch_count(self.handle))
+
+    # ------------------------------------------------------------ CDEF block API
+    def find_direction(self, blocks: np.ndarray, bit_depth: int):
+        blocks = np.ascontiguousarray(blocks, np.uint16).reshape(-1, 64)
+        n = blocks.shape[0]
+        dirs = np.zeros(n, np.uint8)
+        var = np.zeros(n, np.uint32)
+        m = C.c_int32()
+        st = lib().vaco_av1_cdef_find_direction_host(self.handle, ptr(blocks), n, bit_depth, ptr(dirs), ptr(var),
+                                                     C.byref(m))
+        _check(self, st, m)
+        return dirs, var
+
+    def filter_block(self, inputs: np.ndarray, params: np.ndarray) -> np.ndarray:
+        inputs = np.ascontiguousarray(inputs, np.uint16).reshape(-1, 144)
+        params = np.ascontiguousarray(params, abi.cdef_filter_params_dtype())
+        out = np.zeros((inputs.shape[0], 64), np.uint16)
+        m = C.c_int32()
+        st = lib().vaco_av1_cdef_filter_block_host(self.handle, ptr(inputs), ptr(params), inputs.shape[0], ptr(out),
+                                                   C.byref(m))
+        _check(self, st, m)
+        return out
+
+    # ------------------------------------------------------------ frame-level (host arrays)
+    def cdef_picture(self, f: FrameInputs, planes: Optional[Sequence[np.ndarray]] = None) -> List[np.ndarray]:
+        planes = [np.ascontiguousarray(p, np.uint16) for p in (planes if planes is not None else f.planes)]
+        outs = [np.zeros_like(p) for p in planes]
+        shapes = [p.shape for p in planes]
+        src = picture_struct([ptr(p) for p in planes], shapes)
+        dst = picture_struct([ptr(o) for o in outs], shapes)
+        info = f.info()
+        skip = np.ascontiguousarray(f.skip, np.uint8)
+        idx = np.ascontiguousarray(f.cdef_idx, np.int32)
+        params = f.cdef.to_c()
+        m = C.c_int32()
+        st = lib().vaco_av1_cdef_picture_host(self.handle, C.byref(src), C.byref(dst), C.byref(info), ptr(skip),
+                                              ptr(idx), idx.shape[1], idx.size, C.byref(params), C.byref(m))
+        _check(self, st, m)
+        return outs
+
+    def upscale_plane(self, plane: np.ndarray, visible_width: int, output_width: int, height: int,
+                      bit_depth: int) -> np.ndarray:
+        plane = np.ascontiguousarray(plane, np.uint16)
+        out = np.zeros((max(height, 0), max(output_width, 0)), np.uint16)
+        m = C.c_int32()
+        st = lib().vaco_av1_superres_upscale_plane_host(self.handle, ptr(plane), plane.shape[1], plane.shape[0],
+                                                        visible_width, output_width, height, bit_depth,
+                                                        ptr(out) if out.size else None, C.byref(m))
+        _check(self, st, m)
+        return out
+
+    def restore_plane(self, before: np.ndarray, after: np.ndarray, width: int, height: int, bit_depth: int,
+                      unit_size: int, subsampling_y: bool, units: np.ndarray) -> np.ndarray:
+        before = np.ascontiguousarray(before, np.uint16)
+        after = np.ascontiguousarray(after, np.uint16)
+        units = np.ascontiguousarray(units, abi.lr_unit_dtype())
+        cfg = abi.LrPlaneConfig(width, height, bit_depth, unit_size, int(bool(subsampling_y)))
+        out = np.zeros((max(height, 0), max(width, 0)), np.uint16)
+        m = C.c_int32()
+        st = lib().vaco_av1_restore_plane_host(self.handle, ptr(before), before.shape[1], before.shape[0],
+                                               ptr(after), after.shape[1], after.shape[0], C.byref(cfg),
+                                               ptr(units) if len(units) else None, len(units),
+                                               ptr(out) if out.size else None, C.byref(m))
+        _check(self, st, m)
+        return out
+
+    def deblock_picture(self, f: FrameInputs) -> List[np.ndarray]:
+        planes = [np.ascontiguousarray(p, np.uint16) for p in f.planes[: f.num_planes]]
+        outs = [np.zeros_like(p) for p in planes]
+        shapes = [p.shape for p in planes]
+        src = picture_struct([ptr(p) for p in planes], shapes)
+        dst = picture_struct([ptr(o) for o in outs], shapes)
+        info = f.info()
+        params = f.deblock_c()
+        lvl = None if f.lvl_map is None else np.ascontiguousarray(f.lvl_map, np.uint8)
+        txl = np.ascontiguousarray(f.tx_luma, np.uint8)
+        txc = np.ascontiguousarray(f.tx_chroma, np.uint8)
+        m = C.c_int32()
+        st = lib().vaco_av1_deblock_picture_host(self.handle, C.byref(src), C.byref(dst), C.byref(info), ptr(txl),
+                                                 ptr(txc), ptr(lvl), C.byref(params), C.byref(m))
+        _check(self, st, m)
+        return outs
+
+    def postfilter_frame(self, f: FrameInputs) -> List[np.ndarray]:
+        """deblock -> CDEF -> superres -> restoration through the host entry point."""
+        outs = alloc_outputs(f)
+        job = host_job(f, outs)
+        m = C.c_int32()
+        st = lib().vaco_av1_postfilter_frame_host(self.handle, C.byref(job), C.byref(m))
+        _check(self, st, m)
+        return outs
+
+    # ------------------------------------------------------------ device-resident frames
+    def postfilter_frame_dev(self, dev: "DeviceFrame", stream=None) -> None:
+        m = C.c_int32()
+        st = lib().vaco_av1_postfilter_frame_dev(self.handle, stream, C.byref(dev.job), C.byref(m))
+        _check(self, st, m)
+
+
+class DeviceFrame:
+    """A FrameInputs uploaded to device memory (torch tensors) with its output
+    planes allocated, packed as a device-pointer vaco_av1_frame_job."""
+
+    def __init__(self, f: FrameInputs, device: int = 0):
+        import torch
+
+        self.f = f
+        dev = torch.device("cuda", device)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        self.planes = [t(p.view(np.int16)) for p in f.planes[: f.num_planes]]
+        self.outputs = [torch.zeros(f.output_shape(k), dtype=torch.int16, device=dev) for k in range(f.num_planes)]
+        self.side = {k: (t(v) if v is not None else None) for k, v in f.side_arrays().items()}
+        self.units = [t(u.view(np.uint8)) if (k < len(f.lr_units) and f.lr_units[k] is not None) else None
+                      for k in range(3)]
+        side_ptrs = {k: (v.data_ptr() if v is not None else None) for k, v in self.side.items()}
+        unit_ptrs = [u.data_ptr() if u is not None else None for u in self.units]
+        self.job = build_job(f, [p.data_ptr() for p in self.planes], [o.data_ptr() for o in self.outputs],
+                             side_ptrs, unit_ptrs)
+
+    def outputs_numpy(self) -> List[np.ndarray]:
+        return [o.cpu().numpy().view(np.uint16) for o in self.outputs]
