@@ -171,7 +171,7 @@ class DeviceFrame:
         self.planes = [t(p.view(np.int16)) for p in f.planes[: f.num_planes]]
         self.outputs = [torch.zeros(f.output_shape(k), dtype=torch.int16, device=dev) for k in range(f.num_planes)]
         self.side = {k: (t(v) if v is not None else None) for k, v in f.side_arrays().items()}
-        self.units = [t(u.view(np.uint8)) if (k < len(f.lr_units) and f.lr_units[k] is not None) else None
+        self.units = [t(f.lr_units[k].view(np.uint8)) if (k < len(f.lr_units) and f.lr_units[k] is not None) else None
                       for k in range(3)]
         side_ptrs = {k: (v.data_ptr() if v is not None else None) for k, v in self.side.items()}
         unit_ptrs = [u.data_ptr() if u is not None else None for u in self.units]
