@@ -317,9 +317,12 @@ def run_gpu(args, world, rank, local):
         dom_ms = per_stage[dominant]
         achieved = sb[dominant] / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
         traffic = None
-        tp = ROOT / "profiles" / "traffic.json"
+        tp = ROOT / "profiles" / "dram_traffic_per_launch.txt"
         if tp.exists():
-            traffic = json.loads(tp.read_text()).get(args.workload, {}).get(dominant)
+            for ln in tp.read_text().splitlines():
+                parts = ln.split()
+                if len(parts) == 3 and not ln.startswith("#") and parts[0] == args.workload and parts[1] == dominant:
+                    traffic = int(parts[2])
         chain_ms = ms / args.steps
         required = fin + fout + side
         line = {
