@@ -340,6 +340,29 @@ VACO_AV1_API int32_t vaco_av1_postfilter_frame_dev(vaco_av1_ctx* ctx, void* stre
 VACO_AV1_API int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job,
                                        int32_t* msg);
 
+/* The whole chain for callers that cannot call cudaMalloc.  No counterpart in
+ * vaco (vaco allocates every intermediate picture through its Budget).
+ *
+ * Examples of such callers: a decoder plugin in a host application that owns
+ * all device memory through its own pool and forbids plugins from
+ * allocating, or a real-time path where an allocation's implicit device-wide
+ * synchronization would stall unrelated streams.
+ *
+ * The caller passes device pointers for every input and output in `job`.
+ * The call needs no context and allocates nothing.  Intermediate pictures
+ * and the status word live in one fixed device array of 16 MiB (plus 256 B)
+ * in the library; every GPU that loads the library holds it until exit.
+ * Frames whose intermediates do not fit fail with VACO_AV1_LIMIT_EXCEEDED /
+ * VACO_AV1_MSG_SCRATCH_LIMIT.  The array fits up to 1920x1088 4:2:0 without
+ * superres, or 1280x720 with it.
+ * All calls share the array.  Calls whose GPU work overlaps race and produce
+ * undefined output.
+ * The first call on a device resolves the array's address on that device;
+ * make it before any stream capture begins there.
+ * Works on the current device and synchronizes `stream` once. */
+VACO_AV1_API int32_t vaco_av1_postfilter_frame_noalloc(void* stream, const vaco_av1_frame_job* job,
+                                                       int32_t* msg);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

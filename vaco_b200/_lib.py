@@ -38,6 +38,7 @@ SIGNATURES = [
     ("vaco_av1_deblock_picture_host", _i32, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _pi32]),
     ("vaco_av1_postfilter_frame_dev", _i32, [_vp, _vp, _vp, _pi32]),
     ("vaco_av1_postfilter_frame_host", _i32, [_vp, _vp, _pi32]),
+    ("vaco_av1_postfilter_frame_noalloc", _i32, [_vp, _vp, _pi32]),
 ]
 
 _lib = None
