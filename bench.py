@@ -46,7 +46,7 @@ ROTATE_FRAMES = 8  # distinct frames cycled through: > L2 of input planes at 4K
 WORKLOADS = {w.name: (cfg, w) for cfg, w in [(1, synth.CONFIG1), (2, synth.CONFIG2), (2, synth.CONFIG2_DENOM12),
                                                (0, synth.CONFIG0)]}
 METRIC = "AV1 post-filter Mpixel/s at 4K 10-bit (bit-exact); served p50/p99 ms/frame"
-STAGES = ["deblock", "cdef", "superres", "restoration"]
+STAGES = ["deblock_cdef", "unused", "superres", "restoration"]  # vaco_av1_ctx_stage_ms slots
 
 
 def dist_env():
@@ -124,18 +124,28 @@ def frame_bytes(f):
 
 
 def stage_bytes(f):
-    """Algorithmic bytes per launch of each stage as a separate kernel (u16 planes)."""
+    """Algorithmic bytes per launch of each chain kernel (u16 planes).
+
+    deblock_cdef (fused): read the reconstruction once, write the CDEF picture
+    once, plus the transform/level/skip/index side information and the four
+    pre-CDEF rows per stripe boundary that restoration needs.
+    restoration: read the CDEF picture and those boundary rows, write the output.
+    """
     pin = sum(p.size for p in f.planes[: f.num_planes]) * 2
     pout = sum(int(np.prod(f.output_shape(k))) for k in range(f.num_planes)) * 2
-    tx = f.tx_luma.nbytes + f.tx_chroma.nbytes
-    # LR before-image rows actually needed: 4 boundary rows per stripe
-    stripes = (f.coded_height + 8) // 64 + 1
-    boundary = sum(4 * stripes * int(f.output_shape(k)[1]) * 2 for k in range(f.num_planes))
+    side = f.tx_luma.nbytes + f.tx_chroma.nbytes + f.skip.nbytes + f.cdef_idx.nbytes
+    if f.lvl_map is not None:
+        side += f.lvl_map.nbytes
+    boundary = 0
+    for k in range(f.num_planes):
+        rows, cols = f.padded_shape(k)
+        sy = 1 if k else 0
+        boundary += 4 * ((rows + (8 >> sy) + 2) // (64 >> sy) + 1) * cols * 2
     return {
-        "deblock": 2 * pin + tx,                       # read reconstruction, write deblocked
-        "cdef": 2 * pin + f.skip.nbytes + f.cdef_idx.nbytes,
+        "deblock_cdef": 2 * pin + side + boundary,
+        "unused": 0,
         "superres": 0,
-        "restoration": 2 * pout + boundary + sum(u.nbytes for u in f.lr_units),
+        "restoration": pin + pout + boundary + sum(u.nbytes for u in f.lr_units),
     }
 
 

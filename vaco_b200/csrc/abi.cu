@@ -637,6 +637,7 @@ int32_t vaco_av1_restore_plane_dev(vaco_av1_ctx* ctx, void* stream, const uint16
     if (st != VACO_AV1_OK) return st;
     LrPlane p;
     p.before = DevPlaneC{before, before_width, before_height, before_stride};
+    p.before_rows = DevPlaneC{nullptr, 0, 0, 0};
     p.after = DevPlaneC{after, after_width, after_height, after_stride};
     p.out = DevPlane{output, config->width, config->height, out_stride};
     p.width = config->width;
@@ -764,7 +765,9 @@ static bool chain_geometry_ok(const vaco_av1_frame_job* j) {
     return true;
 }
 
-// The chain on device pointers; `d_units` are device copies of the units.
+// The chain on device pointers.  Deblocking and CDEF run fused
+// (dbcdef.cu): the deblocked picture exists only as restoration's compact
+// stripe-boundary rows.
 static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_frame_job* job, int32_t* msg) {
     const vaco_av1_frame_info& info = job->info;
     const int np = info.monochrome ? 1 : 3;
@@ -775,66 +778,114 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
     cudaError_t e = reset_status(ctx, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
 
-    vaco_av1_picture pre, cdef;
-    if (!alloc_picture(ctx, &job->src, np, S_PRE0, &pre, &e)) return cuda_fail(ctx, e, msg);
+    vaco_av1_picture cdef;
     if (!alloc_picture(ctx, &job->src, np, S_CDEF0, &cdef, &e)) return cuda_fail(ctx, e, msg);
+    // Compact pre-CDEF stripe-boundary rows (only restoration reads them).
+    vaco_av1_picture rows_like{}, pre_rows{};
+    DevPlane pre_rows_dp[3] = {};
+    if (lr_active) {
+        for (int k = 0; k < np; ++k) {
+            rows_like.width[k] = job->src.width[k];
+            rows_like.height[k] = pre_rows_count(job->src.height[k], k ? ssy : 0);
+        }
+        if (!alloc_picture(ctx, &rows_like, np, S_PRE0, &pre_rows, &e)) return cuda_fail(ctx, e, msg);
+        for (int k = 0; k < np; ++k) {
+            pre_rows_dp[k] = mplane(pre_rows, k);
+            // rows past the frame bottom are never written; keep them defined
+            e = cudaMemsetAsync(pre_rows.planes[k], 0, (size_t)pre_rows.stride[k] * pre_rows.height[k] * 2, s);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+        }
+    }
     ctx->mark(0, s);
 
-    unsigned long long hk = run_deblock(ctx, s, job->src, pre, info, job->tx_luma, job->tx_chroma, job->lvl_map,
-                                        job->deblock, &e);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
-    ctx->mark(1, s);
-    if (hk == kNoError) {
-        hk = run_cdef(ctx, s, pre, cdef, info, job->skip, job->cdef_idx, job->cdef_stride, job->cdef_count, job->cdef,
-                      &e);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    // ---- deblocking + CDEF (host checks in the order deblock_frame / apply_cdef run them)
+    unsigned long long hk = kNoError;
+    {
+        const vaco_av1_deblock_params& db = job->deblock;
+        bool params_ok = bd_valid(info.bit_depth) && db.sharpness <= 7;
+        for (int k = 0; k < 4; ++k) params_ok = params_ok && db.levels[k] <= 63;
+        if (!params_ok || !job->tx_luma || (np > 1 && !job->tx_chroma))
+            hk = make_key(STAGE_DEBLOCK, 0, params_ok ? VACO_AV1_MSG_NULL_ARGUMENT : VACO_AV1_MSG_DB_PARAMS);
+        const vaco_av1_cdef_params& cp = job->cdef;
+        bool all_zero = true;
+        for (int k = 0; k < 8; ++k)
+            all_zero = all_zero && cp.y_primary[k] == 0 && cp.y_secondary[k] == 0 && cp.uv_primary[k] == 0 &&
+                       cp.uv_secondary[k] == 0;
+        const bool cdef_on = cp.enabled && !all_zero;
+        if (hk == kNoError && cdef_on && (!job->skip || (!job->cdef_idx && job->cdef_count > 0)))
+            hk = make_key(STAGE_CDEF, 0, VACO_AV1_MSG_NULL_ARGUMENT);
+        if (hk == kNoError) {
+            DbCdefLaunch L;
+            L.src = job->src;
+            L.dst = cdef;
+            for (int k = 0; k < 3; ++k) L.pre_rows[k] = k < np && lr_active ? pre_rows_dp[k] : DevPlane{nullptr, 0, 0, 0};
+            L.info = info;
+            L.tx_luma = job->tx_luma;
+            L.tx_chroma = job->tx_chroma;
+            L.lvl_map = job->lvl_map;
+            L.deblock = db;
+            L.skip = cdef_on ? job->skip : nullptr;
+            L.cdef_idx = job->cdef_idx;
+            L.cdef_stride = job->cdef_stride;
+            L.cdef_count = job->cdef_count;
+            L.cdef = cp;
+            L.status = ctx->status;
+            e = launch_dbcdef(L, s);
+            ctx->launches++;
+            if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+        }
     }
+    ctx->mark(1, s);
     ctx->mark(2, s);
-    // Sources for restoration / the visible output.
-    vaco_av1_picture before = pre, after = cdef;
+
+    // ---- superres of the CDEF picture and of the boundary rows
+    vaco_av1_picture after = cdef, before_rows = pre_rows;
     if (hk == kNoError && superres) {
-        vaco_av1_picture out_like{};
+        vaco_av1_picture out_like{}, rows_out_like{};
         for (int k = 0; k < np; ++k) {
-            int sx = k ? ssx : 0, sy = k ? ssy : 0;
+            const int sx = k ? ssx : 0, sy = k ? ssy : 0;
             out_like.width[k] = (info.upscaled_width + sx) >> sx;
             out_like.height[k] = (info.coded_height + sy) >> sy;
+            rows_out_like.width[k] = out_like.width[k];
+            rows_out_like.height[k] = pre_rows.height[k];
         }
-        vaco_av1_picture ucdef, upre;
+        vaco_av1_picture ucdef, urows;
         if (!alloc_picture(ctx, &out_like, np, S_UCDEF0, &ucdef, &e)) return cuda_fail(ctx, e, msg);
-        SuperresPlane sp[6];
-        int n = 0;
+        SuperresPlane sp[3];
         for (int k = 0; k < np; ++k) {
-            int sx = k ? ssx : 0, sy = k ? ssy : 0;
-            SuperresPlane& p = sp[n++];
-            p.in = cplane(cdef, k);
-            p.out = mplane(ucdef, k);
-            p.visible_width = (info.coded_width + sx) >> sx;
-            p.output_width = (info.upscaled_width + sx) >> sx;
-            p.height = (info.coded_height + sy) >> sy;
+            const int sx = k ? ssx : 0, sy = k ? ssy : 0;
+            sp[k].in = cplane(cdef, k);
+            sp[k].out = mplane(ucdef, k);
+            sp[k].visible_width = (info.coded_width + sx) >> sx;
+            sp[k].output_width = (info.upscaled_width + sx) >> sx;
+            sp[k].height = (info.coded_height + sy) >> sy;
         }
-        e = launch_superres(sp, n, info.bit_depth, ctx->status, STAGE_SUPERRES, s);
+        e = launch_superres(sp, np, info.bit_depth, ctx->status, STAGE_SUPERRES, s);
         ctx->launches++;
         if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
         after = ucdef;
         if (lr_active) {
-            if (!alloc_picture(ctx, &out_like, np, S_UPRE0, &upre, &e)) return cuda_fail(ctx, e, msg);
+            if (!alloc_picture(ctx, &rows_out_like, np, S_UPRE0, &urows, &e)) return cuda_fail(ctx, e, msg);
             for (int k = 0; k < np; ++k) {
-                sp[k].in = cplane(pre, k);
-                sp[k].out = mplane(upre, k);
+                sp[k].in = cplane(pre_rows, k);
+                sp[k].out = mplane(urows, k);
+                sp[k].height = pre_rows.height[k];
             }
             e = launch_superres(sp, np, info.bit_depth, ctx->status, STAGE_SUPERRES, s);
             ctx->launches++;
             if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
-            before = upre;
+            before_rows = urows;
         }
     }
     ctx->mark(3, s);
+
+    // ---- restoration (or the visible copy) into the output
     if (hk == kNoError) {
         LrPlane lp[3];
         int nlr = 0;
         for (int k = 0; k < np && hk == kNoError; ++k) {
-            int sx = k ? ssx : 0, sy = k ? ssy : 0;
-            int w = info.upscaled_width >> sx, h = info.coded_height >> sy;
+            const int sx = k ? ssx : 0, sy = k ? ssy : 0;
+            const int w = info.upscaled_width >> sx, h = info.coded_height >> sy;
             if (job->lr_type[k] == VACO_AV1_FRAME_LR_NONE) {
                 // copy_visible_plane (decode.rs:673-681)
                 e = cudaMemcpy2DAsync(job->dst.planes[k], (size_t)job->dst.stride[k] * 2, after.planes[k],
@@ -848,7 +899,7 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
             }
             vaco_av1_lr_plane_config c{w, h, info.bit_depth, job->lr_unit_size[k], (k && ssy) ? 1 : 0};
             int cols = 0, rows = 0;
-            hk = lr_host_checks(k, &c, before.width[k], before.height[k], after.width[k], after.height[k],
+            hk = lr_host_checks(k, &c, after.width[k], after.height[k], after.width[k], after.height[k],
                                 job->lr_unit_count[k], &cols, &rows);
             if (hk != kNoError) break;
             if (!job->lr_units[k]) {
@@ -859,7 +910,8 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
             ctx->launches++;
             if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
             LrPlane& p = lp[nlr++];
-            p.before = cplane(before, k);
+            p.before = DevPlaneC{nullptr, 0, 0, 0};
+            p.before_rows = cplane(before_rows, k);
             p.after = cplane(after, k);
             p.out = mplane(job->dst, k);
             p.width = w;

@@ -12,6 +12,7 @@
 // maximum masks it out, which is exactly vaco's "unavailable border samples
 // are ignored" rule (the availability edges of apply_cdef are the plane
 // bounds, decode.rs:828-831).
+#include "cdef_core.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -19,149 +20,7 @@ namespace vaco {
 
 namespace {
 
-constexpr int kSent = 0xC000;      // > any 12-bit sample; & kMaxMask == 0
-constexpr int kMaxMask = 0x3FFF;
-
-// (row, col) step per direction and distance (src/cdef.rs:57-66).
-__constant__ int8_t c_dir[8][2][2] = {
-    {{-1, 1}, {-2, 2}}, {{0, 1}, {-1, 2}}, {{0, 1}, {0, 2}},  {{0, 1}, {1, 2}},
-    {{1, 1}, {2, 2}},   {{1, 0}, {2, 1}},  {{1, 0}, {2, 0}},  {{1, 0}, {2, -1}},
-};
-
-// Line index of pixel (i, j) for direction d (src/cdef.rs:88-97).
-__host__ __device__ constexpr int dir_bin(int d, int i, int j) {
-    return d == 0 ? i + j : d == 1 ? i + j / 2 : d == 2 ? i : d == 3 ? 3 + i - j / 2
-         : d == 4 ? 7 + i - j : d == 5 ? 3 + j - i / 2 : d == 6 ? j : i / 2 + j;
-}
-__host__ __device__ constexpr int dir_count(int d, int b) {
-    int n = 0;
-    for (int i = 0; i < 8; ++i)
-        for (int j = 0; j < 8; ++j) n += dir_bin(d, i, j) == b;
-    return n;
-}
-__host__ __device__ constexpr int dir_weight(int d, int b) {
-    return dir_count(d, b) ? 840 / dir_count(d, b) : 0;
-}
-
-// Costs of directions P and P+4 for one 8x8 block at `blk` (row pitch in
-// samples, rows 16-byte aligned).  Fully unrolled: every bin is a register.
-template <int P>
-__device__ __forceinline__ void dir_costs(const uint16_t* blk, int pitch, int shift, int& c_lo, int& c_hi) {
-    int a[15], b[15];
-#pragma unroll
-    for (int k = 0; k < 15; ++k) a[k] = b[k] = 0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        uint4 row = *reinterpret_cast<const uint4*>(blk + i * pitch);
-        uint32_t w[4] = {row.x, row.y, row.z, row.w};
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            int s = (j & 1) ? (w[j >> 1] >> 16) : (w[j >> 1] & 0xFFFF);
-            int v = (s >> shift) - 128;
-            a[dir_bin(P, i, j)] += v;
-            b[dir_bin(P + 4, i, j)] += v;
-        }
-    }
-    int lo = 0, hi = 0;
-#pragma unroll
-    for (int k = 0; k < 15; ++k) {
-        if (dir_weight(P, k)) lo += a[k] * a[k] * dir_weight(P, k);
-        if (dir_weight(P + 4, k)) hi += b[k] * b[k] * dir_weight(P + 4, k);
-    }
-    c_lo = lo;
-    c_hi = hi;
-}
-
-__device__ __forceinline__ void dir_costs_pair(int pair, const uint16_t* blk, int pitch, int shift, int& lo, int& hi) {
-    switch (pair) {
-        case 0: dir_costs<0>(blk, pitch, shift, lo, hi); break;
-        case 1: dir_costs<1>(blk, pitch, shift, lo, hi); break;
-        case 2: dir_costs<2>(blk, pitch, shift, lo, hi); break;
-        default: dir_costs<3>(blk, pitch, shift, lo, hi); break;
-    }
-}
-
-__device__ __forceinline__ void best_direction(const int* cost8, int& best, uint32_t& var) {
-    int b = 0;
-#pragma unroll
-    for (int d = 1; d < 8; ++d)
-        if (cost8[d] > cost8[b]) b = d;
-    best = b;
-    var = (uint32_t)((cost8[b] - cost8[(b + 4) & 7]) >> 10);
-}
-
-// constrain (src/cdef.rs:126-133); threshold 0 yields 0 for any shift.
-__device__ __forceinline__ int constrain(int d, int t, int shift) {
-    int a = abs(d);
-    int c = min(a, max(0, t - (a >> shift)));
-    return d < 0 ? -c : c;
-}
-
-__device__ __forceinline__ int ilog2u(unsigned v) { return 31 - __clz(v); }
-
-// adjust_strength (src/cdef.rs:209-220).
-__device__ __forceinline__ int adjust_strength(int primary, uint32_t variance) {
-    if (variance == 0) return 0;
-    uint32_t scaled = variance >> 6;
-    uint32_t lg = scaled == 0 ? 0 : min((uint32_t)ilog2u(scaled), 12u);
-    return (int)(((uint32_t)primary * (4 + lg) + 8) >> 4);
-}
-
-// chroma_direction (src/cdef.rs:224-230).
-__device__ __forceinline__ int chroma_direction(int d, int sx, int sy) {
-    const uint32_t k10 = 0x66654207u;  // nibbles of [7,0,2,4,5,6,6,6]
-    const uint32_t k01 = 0x06432221u;  // nibbles of [1,2,2,2,3,4,6,0]
-    if (sx && !sy) return (k10 >> (4 * (d & 7))) & 0xF;
-    if (!sx && sy) return (k01 >> (4 * (d & 7))) & 0xF;
-    return d & 7;
-}
-
-// Per-block filter parameters, offsets in shared-memory samples.
-struct BlockFilter {
-    int off[6];   // primary d0,d1; secondary (dir+2) d0,d1; secondary (dir+6) d0,d1
-    short pri, sec;
-    uint8_t pri_shift, sec_shift, pt0, pt1;
-};
-
-__device__ __forceinline__ BlockFilter make_filter(int dir, int pri, int sec, int damping, int shift, int pitch) {
-    BlockFilter f;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        f.off[k] = c_dir[dir][k][0] * pitch + c_dir[dir][k][1];
-        f.off[2 + k] = c_dir[(dir + 2) & 7][k][0] * pitch + c_dir[(dir + 2) & 7][k][1];
-        f.off[4 + k] = c_dir[(dir + 6) & 7][k][0] * pitch + c_dir[(dir + 6) & 7][k][1];
-    }
-    f.pri = (short)pri;
-    f.sec = (short)sec;
-    f.pri_shift = (uint8_t)(pri ? max(0, damping - ilog2u(pri)) : 0);
-    f.sec_shift = (uint8_t)(sec ? max(0, damping - ilog2u(sec)) : 0);
-    bool odd = ((pri >> shift) & 1) != 0;
-    f.pt0 = odd ? 3 : 4;
-    f.pt1 = odd ? 3 : 2;
-    return f;
-}
-
-// One output sample of filter_block (src/cdef.rs:167-202) at smem position s.
-__device__ __forceinline__ int filter_px(const uint16_t* s, const BlockFilter& f) {
-    const int cur = s[0];
-    int mn = cur, mx = cur, sum = 0;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        const int ptap = k ? f.pt1 : f.pt0;
-        const int stap = 2 - k;
-        int p0 = s[f.off[k]], p1 = s[-f.off[k]];
-        int s0 = s[f.off[2 + k]], s1 = s[-f.off[2 + k]];
-        int s2 = s[f.off[4 + k]], s3 = s[-f.off[4 + k]];
-        mn = min(mn, min(min(p0, p1), min(min(s0, s1), min(s2, s3))));
-        mx = max(mx, max(max(p0 & kMaxMask, p1 & kMaxMask),
-                         max(max(s0 & kMaxMask, s1 & kMaxMask), max(s2 & kMaxMask, s3 & kMaxMask))));
-        sum += ptap * (constrain(p0 - cur, f.pri, f.pri_shift) + constrain(p1 - cur, f.pri, f.pri_shift));
-        sum += stap * (constrain(s0 - cur, f.sec, f.sec_shift) + constrain(s1 - cur, f.sec, f.sec_shift) +
-                       constrain(s2 - cur, f.sec, f.sec_shift) + constrain(s3 - cur, f.sec, f.sec_shift));
-    }
-    int v = cur + ((8 + sum - (sum < 0)) >> 4);
-    return min(max(v, mn), mx);
-}
+using namespace cdefk;
 
 // ---------------------------------------------------------------- frame kernel
 
@@ -375,56 +234,48 @@ __global__ void __launch_bounds__(kThreads) cdef_frame_kernel(CdefFrameArgs a) {
         if (!a.bd_ok) return;
     }
 
-    // Luma: thread -> block tid/4, rows 2*(tid%4) .. +1, 8 samples each.
-    {
-        const int b = tid >> 2, by = b >> 3, bx = b & 7;
-        const DevPlane& d = a.dst[0];
-        const int gx = x0 + bx * 8;
-        if (gx < d.width) {
-            const bool act = s_active[b];
-            BlockFilter f;
-            if (act) f = s_filter[0][b];
+    // Filtering: one lane per column and warps walking contiguous rows, so the
+    // taps of a warp read consecutive shared-memory samples (no bank
+    // conflicts) and every output row is one coalesced store.  Each lane
+    // handles whole block columns: the tap addresses of a block are formed
+    // once and the rows inside the block use immediate offsets.
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int p = 0; p < a.num_planes; ++p) {
+        const int sx = p ? a.ssx : 0, sy = p ? a.ssy : 0;
+        const int tw = 64 >> sx, th = 64 >> sy;   // tile extent in this plane
+        const int bw = 8 >> sx, bh = 8 >> sy;     // block extent
+        const int pitch = p ? cpitch : kLumaPitch;
+        const DevPlane& d = a.dst[p];
+        const int px0 = p ? x0 >> a.ssx : x0, py0 = p ? y0 >> a.ssy : y0;
+        const int strips = tw >> 5;               // 32-column strips (2 or 1)
+        const int wps = (kThreads / 32) / strips; // warps per strip
+        const int rpw = th / wps;                 // rows per warp (a multiple of bh)
+        const int c = (warp / wps) * 32 + lane;   // tile column of this lane
+        const int gx = px0 + c, bx = c / bw;
+        const bool col_in = gx < d.width;
+        for (int r0 = (warp % wps) * rpw; r0 < (warp % wps + 1) * rpw; r0 += bh) {
+            if (py0 + r0 >= d.height) break;
+            const int b = (r0 / bh) * 8 + bx;
+            const uint16_t* s = tile[p] + (2 + r0) * pitch + 8 + c;
+            uint16_t* o = d.data + (long)(py0 + r0) * d.stride + gx;
+            const int rows = min(bh, d.height - (py0 + r0));
+            if (s_active[b]) {
+                const BlockFilter f = s_filter[p][b];
+                if (bh == 8) {
 #pragma unroll
-            for (int rr = 0; rr < 2; ++rr) {
-                const int row = (tid & 3) * 2 + rr;
-                const int gy = y0 + by * 8 + row;
-                if (gy >= d.height) continue;
-                const uint16_t* s = tile[0] + (2 + by * 8 + row) * kLumaPitch + 8 + bx * 8;
-                uint32_t out[4];
-#pragma unroll
-                for (int j = 0; j < 8; j += 2) {
-                    int v0 = act ? filter_px(s + j, f) : s[j];
-                    int v1 = act ? filter_px(s + j + 1, f) : s[j + 1];
-                    out[j >> 1] = (uint32_t)v0 | ((uint32_t)v1 << 16);
-                }
-                uint16_t* o = d.data + (long)gy * d.stride + gx;
-                if (vec) {
-                    *reinterpret_cast<uint4*>(o) = make_uint4(out[0], out[1], out[2], out[3]);
+                    for (int j = 0; j < 8; ++j) {
+                        const int v = filter_px(s + j * pitch, f);
+                        if (col_in && j < rows) o[(long)j * d.stride] = (uint16_t)v;
+                    }
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) o[j] = (uint16_t)(out[j >> 1] >> (16 * (j & 1)));
+                    for (int j = 0; j < 4; ++j) {
+                        const int v = filter_px(s + j * pitch, f);
+                        if (col_in && j < rows) o[(long)j * d.stride] = (uint16_t)v;
+                    }
                 }
-            }
-        }
-    }
-    // Chroma: items are (block, row) pairs of (8>>ssx)-sample rows.
-    for (int p = 1; p < a.num_planes; ++p) {
-        const int bw = 8 >> a.ssx, bh = 8 >> a.ssy;
-        const DevPlane& d = a.dst[p];
-        const int px0 = x0 >> a.ssx, py0 = y0 >> a.ssy;
-        for (int item = tid; item < 64 * bh; item += kThreads) {
-            const int b = item / bh, row = item - b * bh;
-            const int by = b >> 3, bx = b & 7;
-            const int gx = px0 + bx * bw, gy = py0 + by * bh + row;
-            if (gx >= d.width || gy >= d.height) continue;
-            const bool act = s_active[b];
-            const uint16_t* s = tile[p] + (2 + by * bh + row) * cpitch + 8 + bx * bw;
-            uint16_t* o = d.data + (long)gy * d.stride + gx;
-            if (act) {
-                const BlockFilter f = s_filter[p][b];
-                for (int j = 0; j < bw; ++j) o[j] = (uint16_t)filter_px(s + j, f);
-            } else {
-                for (int j = 0; j < bw; ++j) o[j] = s[j];
+            } else if (col_in) {
+                for (int j = 0; j < rows; ++j) o[(long)j * d.stride] = s[j * pitch];
             }
         }
     }

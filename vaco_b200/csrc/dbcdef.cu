@@ -1,0 +1,529 @@
+// dbcdef.cu -- deblocking (AV1 7.14) fused with CDEF (vaco src/decode.rs:739-862)
+// in one pass over each 64x64 filter block.
+//
+// Why fused: the chain needs the deblocked picture only (a) as CDEF's input
+// and (b) as restoration's pre-CDEF source, which restoration reads at just
+// four rows around every stripe boundary (src/restoration.rs:233-244).  One
+// CTA therefore stages its tile with a 16-sample halo, runs both deblocking
+// passes in shared memory (all vertical edges of the staged region, then the
+// horizontal edges that reach the CDEF window), writes the stripe-boundary
+// rows to a compact buffer, and filters CDEF straight from the deblocked tile.
+// The deblocked picture never round-trips through HBM.
+//
+// Halo arithmetic (plane units, tile [x0, x0+tw) x [y0, y0+th)):
+//   CDEF reads the deblocked window [x0-2, x0+tw+2) x [y0-2, y0+th+2).
+//   Horizontal edges that modify window rows: E in [y0-4, y0+th+4] (a 14-tap
+//   filter modifies E-6..E+5); they read rows [E-7, E+6], i.e. [y0-11, y0+th+10].
+//   Vertical edges that modify window columns: X in [x0-4, x0+tw+4]; they read
+//   columns [x0-11, x0+tw+10].  The vertical pass runs on rows [y0-12,
+//   y0+th+12), which covers every row the horizontal pass reads.
+// The staged region is [x0-16, x0+tw+16) x [y0-16, y0+th+16).
+// Within a pass no two edges touch a common sample (see deblock.cu), so both
+// passes run one thread per edge line, in place; reads past the plane repeat
+// the edge sample and writes past it are dropped, as in deblock.cu.
+#include <algorithm>
+
+#include "cdef_core.cuh"
+#include "common.cuh"
+#include "deblock_core.cuh"
+#include "kernels.cuh"
+
+namespace vaco {
+
+namespace {
+
+using namespace cdefk;
+using namespace dbk;
+
+constexpr int kThreads = 256;
+constexpr int kHalo = 16;
+// Segments per pass and plane are at most (th/4+4) x (tw/4+3) = 380.  Size
+// class lists: 0 = size 4 (any plane, up to 3 x 380), 1 = chroma size 8
+// (2 x 380), 2 = luma size 8 (380), 3 = luma size 16 (380).
+__constant__ int c_list_off[4] = {0, 1140, 1900, 2280};
+constexpr int kListTotal = 2660;
+
+struct PlaneGeom {
+    int tw, th;        // tile extent in this plane
+    int pitch, rows;   // staged region
+    int sx, sy;
+};
+
+__device__ __forceinline__ PlaneGeom plane_geom(int p, int ssx, int ssy) {
+    PlaneGeom g;
+    g.sx = p ? ssx : 0;
+    g.sy = p ? ssy : 0;
+    g.tw = 64 >> g.sx;
+    g.th = 64 >> g.sy;
+    g.pitch = g.tw + 2 * kHalo;
+    g.rows = g.th + 2 * kHalo;
+    return g;
+}
+
+struct DbCdefArgs {
+    DevPlaneC src[3];
+    DevPlane dst[3];            // CDEF output planes
+    DevPlane pre_rows[3];       // stripe-boundary rows of the deblocked picture (may be null)
+    int num_planes, ssx, ssy, bit_depth, shift;
+    int mi_rows, mi_cols, coded_width, coded_height;
+    // deblocking
+    const uint8_t* tx_luma;
+    const uint8_t* tx_chroma;
+    const uint8_t* lvl_map;
+    uint8_t levels[4];
+    int sharpness;
+    int deblock_on;
+    // CDEF
+    int cdef_on;
+    const uint8_t* skip;
+    const int32_t* cdef_idx;
+    int cdef_stride, cdef_count;
+    int damping;
+    uint8_t y_pri[8], y_sec[8], uv_pri[8], uv_sec[8];
+    DeviceStatus* status;
+    int vec_ok;
+    size_t plane_off[3];        // shared-memory offset (samples) of each staged plane
+};
+
+// CDEF output of one plane tile from the staged (deblocked) samples: warp w
+// filters block row w; lane l owns pixel pairs at tile column 2*(l % ppr),
+// rows l / ppr + RPI*j.  PITCH is the staged pitch, BH the block height.
+template <int PITCH, int BH, int RPI>
+__device__ __forceinline__ void filter_pairs(const uint16_t* t, const DevPlane& d, int px0, int py0, int tw,
+                                             const uint8_t* active, const PairBlock* blocks, bool edge, int warp,
+                                             int lane, int sx) {
+    const int ppr = 32 / RPI;              // pairs per row
+    const int lp = lane % ppr, lr = lane / ppr;
+    const int x = 2 * lp;
+    if (x >= tw) return;
+    const int bx = x >> (3 - sx);
+    const int gx = px0 + x;
+    const bool col_in = gx < d.width;
+    const int br = warp;                   // 8 block rows, 8 warps
+    const int r0 = br * BH;
+    if (py0 + r0 >= d.height) return;
+    const int rows_here = min(BH, d.height - (py0 + r0));
+    const int b = br * 8 + bx;
+    const int base_i = (kHalo + r0 + lr) * PITCH + kHalo + x;  // left sample, first row of this lane
+    uint32_t* o = reinterpret_cast<uint32_t*>(d.data + (long)(py0 + r0 + lr) * d.stride + gx);
+    const long ostride = (long)d.stride * RPI / 2;  // words per RPI rows
+    if (active[b]) {
+        const PairBlock f = blocks[b];
+        PairTap taps[12];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            taps[2 * k] = pair_tap(t, base_i + f.off[k]);
+            taps[2 * k + 1] = pair_tap(t, base_i - f.off[k]);
+        }
+        const uint32_t* cw = reinterpret_cast<const uint32_t*>(t + base_i);
+#pragma unroll
+        for (int j = 0; j < BH / RPI; ++j) {
+            const int rr = lr + RPI * j;
+            const int woff = j * RPI * PITCH / 2;
+            const uint32_t cur = cw[woff];
+            const uint32_t v = edge ? filter_pair<true>(cur, taps, woff, f) : filter_pair<false>(cur, taps, woff, f);
+            if (col_in && rr < rows_here) o[j * ostride] = v;
+        }
+    } else if (col_in) {
+        const uint32_t* cw = reinterpret_cast<const uint32_t*>(t + base_i);
+#pragma unroll
+        for (int j = 0; j < BH / RPI; ++j)
+            if (lr + RPI * j < rows_here) o[j * ostride] = cw[j * RPI * PITCH / 2];
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 4) dbcdef_kernel(DbCdefArgs a) {
+    extern __shared__ __align__(16) uint16_t smem[];
+    __shared__ int s_cost[64][8];
+    __shared__ PairBlock s_pair[3][64];
+    __shared__ uint8_t s_active[64];
+    __shared__ uint32_t s_list[kListTotal];  // per size class: plane<<28 | segment<<8 | level
+    __shared__ int s_count[4];
+    __shared__ int s_any, s_bad;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int mi_r0 = blockIdx.y * 16, mi_c0 = blockIdx.x * 16;
+    const int x0 = mi_c0 * 4, y0 = mi_r0 * 4;
+    const int maxv = (1 << a.bit_depth) - 1;
+
+    // ---- CDEF block activity (decode.rs:772-779)
+    const long slot = (long)(mi_r0 >> 4) * a.cdef_stride + (mi_c0 >> 4);
+    const int index = (a.cdef_on && slot < a.cdef_count) ? __ldg(a.cdef_idx + slot) : -1;
+    if (tid == 0) {
+        s_any = 0;
+        s_bad = 0;
+    }
+    __syncthreads();
+    if (tid < 64) {
+        const int r = mi_r0 + (tid >> 3) * 2, c = mi_c0 + (tid & 7) * 2;
+        bool act = false;
+        if (r < a.mi_rows && c < a.mi_cols && index >= 0) {
+            auto sk = [&](int rr, int cc) {
+                return rr < a.mi_rows && cc < a.mi_cols && a.skip[(long)rr * a.mi_cols + cc] != 0;
+            };
+            act = !(sk(r, c) && sk(r + 1, c) && sk(r, c + 1) && sk(r + 1, c + 1));
+        }
+        s_active[tid] = act;
+        if (act) s_any = 1;
+    }
+
+    // ---- deblocking side-information checks for this tile's own cells
+    {
+        int bad = 0;
+        for (int i = tid; i < 256; i += kThreads) {
+            const int r = mi_r0 + (i >> 4), c = mi_c0 + (i & 15);
+            if (r < a.mi_rows && c < a.mi_cols) {
+                const long cell = (long)r * a.mi_cols + c;
+                bad |= __ldg(a.tx_luma + cell) > 18;
+                if (a.lvl_map) {
+                    const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(a.lvl_map) + cell);
+                    bad |= ((w & 0xFF) > 63) | (((w >> 8) & 0xFF) > 63) | (((w >> 16) & 0xFF) > 63) | ((w >> 24) > 63);
+                }
+            }
+        }
+        if (a.num_planes > 1) {
+            const int ccols = (a.mi_cols + a.ssx) >> a.ssx, crows = (a.mi_rows + a.ssy) >> a.ssy;
+            const int cw = 16 >> a.ssx, ch = 16 >> a.ssy;
+            for (int i = tid; i < cw * ch; i += kThreads) {
+                const int r = (mi_r0 >> a.ssy) + i / cw, c = (mi_c0 >> a.ssx) + i % cw;
+                if (r < crows && c < ccols) bad |= __ldg(a.tx_chroma + (long)r * ccols + c) > 18;
+            }
+        }
+        if (bad) report_error(a.status, STAGE_DEBLOCK, 0, VACO_AV1_MSG_DB_PARAMS);
+    }
+
+    // ---- stage every plane with a 16-sample halo (edge-clamped) and check samples
+    {
+        int bad = 0;
+        for (int p = 0; p < a.num_planes; ++p) {
+            const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+            const DevPlaneC& P = a.src[p];
+            uint16_t* t = smem + a.plane_off[p];
+            const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+            const int vpr = g.pitch / 8;
+            for (int v = tid; v < g.rows * vpr; v += kThreads) {
+                const int r = v / vpr, cv = v - r * vpr;
+                const int y = clampi(py0 - kHalo + r, 0, P.height - 1);
+                const int x = px0 - kHalo + cv * 8;
+                const bool interior_row = (py0 - kHalo + r) == y && y >= py0 && y < py0 + g.th;
+                const uint16_t* row = P.data + (long)y * P.stride;
+                uint16_t* d = t + r * g.pitch + cv * 8;
+                if (a.vec_ok && x >= 0 && x + 8 <= P.width) {
+                    const uint4 q = __ldg(reinterpret_cast<const uint4*>(row + x));
+                    *reinterpret_cast<uint4*>(d) = q;
+                    if (interior_row && x >= px0 && x < px0 + g.tw) {
+                        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            bad |= ((int)(w[k] & 0xFFFF) > maxv) | ((int)(w[k] >> 16) > maxv);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const int xx = x + k;
+                        const int s = __ldg(row + clampi(xx, 0, P.width - 1));
+                        d[k] = (uint16_t)s;
+                        if (interior_row && xx >= px0 && xx < px0 + g.tw && xx < P.width) bad |= s > maxv;
+                    }
+                }
+            }
+        }
+        if (bad) report_error(a.status, STAGE_DEBLOCK, 1, VACO_AV1_MSG_DB_SAMPLE);
+    }
+    __syncthreads();
+
+    // ---- deblocking, pass 0 (vertical edges) then pass 1 (horizontal edges)
+    //
+    // Per pass, every 4-sample edge segment of the needed region gets its
+    // decision (7.14.2-7.14.5: on screen, transform edge, filter size, level)
+    // and is appended to the list of its size class; the lists are then
+    // filtered one class at a time (4 lanes per segment, one per line), so a
+    // warp never mixes the 4-, 6-, 8- and 14-tap code paths.
+    //   pass 0 segments: rows [py0-8, py0+th+8) in 4-row cells x edges
+    //                    X = px0-4+4e, e < tw/4+3
+    //   pass 1 segments: edges E = py0-4+4e, e < th/4+3 x 4-column cells from
+    //                    px0-4, covering columns [px0-2, px0+tw+2)
+    // The horizontal edges read rows [E-7, E+6] only where their filter is
+    // 14 taps (E a multiple of 16), so [py0-7, py0+th+6] bounds every read.
+    if (a.deblock_on) {
+        for (int pass = 0; pass < 2; ++pass) {
+            if (tid < 4) s_count[tid] = 0;
+            __syncthreads();
+            for (int p = 0; p < a.num_planes; ++p) {
+                if (p != 0 && a.levels[1 + p] == 0) continue;
+                const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+                const DevPlane& P = a.dst[p];
+                const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+                const uint8_t* map = p ? a.tx_chroma : a.tx_luma;
+                const int map_cols = p ? (a.mi_cols + a.ssx) >> a.ssx : a.mi_cols;
+                const int n_a = pass == 0 ? g.th / 4 + 4 : g.th / 4 + 3;
+                const int n_b = pass == 0 ? g.tw / 4 + 3 : g.tw / 4 + 2;
+                for (int i = tid; i < n_a * n_b; i += kThreads) {
+                    const int ia = i / n_b, ib = i - ia * n_b;
+                    const int yp = pass == 0 ? py0 - 8 + 4 * ia : py0 - 4 + 4 * ia;
+                    const int xp = px0 - 4 + 4 * ib;
+                    const int col = (xp >> 2) << g.sx, row = (yp >> 2) << g.sy;
+                    const bool on_screen = xp >= 0 && yp >= 0 && xp < P.width && yp < P.height &&
+                                           col * 4 < a.coded_width && row * 4 < a.coded_height &&
+                                           (pass == 0 ? xp > 0 : yp > 0);
+                    if (!on_screen) continue;
+                    const int cur = map[(long)(yp >> 2) * map_cols + (xp >> 2)];
+                    const int prev = pass == 0 ? map[(long)(yp >> 2) * map_cols + (xp >> 2) - 1]
+                                               : map[(long)((yp >> 2) - 1) * map_cols + (xp >> 2)];
+                    const int cl = pass == 0 ? tx_w_log2(cur) : tx_h_log2(cur);
+                    const int pl = pass == 0 ? tx_w_log2(prev) : tx_h_log2(prev);
+                    if (((pass == 0 ? xp : yp) & ((1 << cl) - 1)) != 0) continue;
+                    const int size = min(p ? 8 : 16, 1 << min(cl, pl));
+                    const int r = row | g.sy, c = col | g.sx;
+                    const int li = p == 0 ? pass : p + 1;  // level index (7.14.5)
+                    int lvl;
+                    if (a.lvl_map) {
+                        lvl = __ldg(a.lvl_map + ((long)r * a.mi_cols + c) * 4 + li);
+                        if (lvl == 0) {
+                            const int pr = pass == 0 ? r : r - (1 << g.sy);
+                            const int pc = pass == 0 ? c - (1 << g.sx) : c;
+                            lvl = __ldg(a.lvl_map + ((long)pr * a.mi_cols + pc) * 4 + li);
+                        }
+                    } else {
+                        lvl = a.levels[li];
+                    }
+                    if (lvl == 0) continue;
+                    const int cls = size == 4 ? 0 : p ? 1 : size == 8 ? 2 : 3;
+                    const int at = atomicAdd(&s_count[cls], 1);
+                    s_list[c_list_off[cls] + at] = (uint32_t)((p << 28) | (i << 8) | lvl);
+                }
+            }
+            __syncthreads();
+            for (int cls = 0; cls < 4; ++cls) {
+                const int count = s_count[cls];
+                for (int item = tid; item < count * 4; item += kThreads) {
+                    const uint32_t e = s_list[c_list_off[cls] + (item >> 2)];
+                    const int line = item & 3, p = e >> 28, i = (e >> 8) & 0xFFFFF, lvl = e & 0xFF;
+                    const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+                    const DevPlane& P = a.dst[p];
+                    const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+                    uint16_t* t = smem + a.plane_off[p];
+                    const Strength s = strength_of(lvl, a.sharpness);
+                    if (pass == 0) {
+                        const int n_b = g.tw / 4 + 3;
+                        const int ia = i / n_b, ib = i - ia * n_b;
+                        const int yp = py0 - 8 + 4 * ia + line, xp = px0 - 4 + 4 * ib;
+                        uint16_t* q = t + (yp - py0 + kHalo) * g.pitch + (xp - px0 + kHalo);
+                        const int nq = P.width - xp, np = xp;
+                        if (cls == 0) line_size4<1>(q, 1, nq, np, s, a.bit_depth);
+                        else if (cls == 1) line_size6<1>(q, 1, nq, np, s, a.bit_depth);
+                        else if (cls == 2) line_size8<1>(q, 1, nq, np, s, a.bit_depth);
+                        else line_size16<1>(q, 1, nq, np, s, a.bit_depth);
+                    } else {
+                        const int n_b = g.tw / 4 + 2;
+                        const int ia = i / n_b, ib = i - ia * n_b;
+                        const int yp = py0 - 4 + 4 * ia, xp = px0 - 4 + 4 * ib + line;
+                        if (xp < px0 - 2 || xp >= px0 + g.tw + 2 || xp >= P.width) continue;
+                        uint16_t* q = t + (yp - py0 + kHalo) * g.pitch + (xp - px0 + kHalo);
+                        const int nq = P.height - yp, np = yp;
+                        if (g.pitch == 96) {
+                            if (cls == 0) line_size4<96>(q, 96, nq, np, s, a.bit_depth);
+                            else if (cls == 1) line_size6<96>(q, 96, nq, np, s, a.bit_depth);
+                            else if (cls == 2) line_size8<96>(q, 96, nq, np, s, a.bit_depth);
+                            else line_size16<96>(q, 96, nq, np, s, a.bit_depth);
+                        } else {
+                            if (cls == 0) line_size4<0>(q, g.pitch, nq, np, s, a.bit_depth);
+                            else line_size6<0>(q, g.pitch, nq, np, s, a.bit_depth);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+
+    // ---- stripe-boundary rows of the deblocked picture for restoration:
+    // rows y with (y + offset + 2) mod stripe < 4, stored at 4*boundary + that
+    // remainder (boundary = (y + offset + 2) / stripe >= 1).
+    for (int p = 0; p < a.num_planes; ++p) {
+        const DevPlane& R = a.pre_rows[p];
+        if (!R.data) continue;
+        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        const int sh = 64 >> g.sy, off = 8 >> g.sy;
+        const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+        const uint16_t* src = smem + a.plane_off[p];
+        const int width = a.dst[p].width, height = a.dst[p].height;
+        // the tile (th rows, th a multiple of the stripe height or half of it)
+        // holds boundary rows y = k*sh - off - 2 + sub, sub < 4
+        for (int i = warp; i < 4 * (g.th / sh + 1); i += kThreads / 32) {
+            const int kk = i >> 2, sub = i & 3;
+            const int kb = (py0 + off + 2) / sh + kk;
+            const int y = kb * sh - off - 2 + sub;
+            if (kb < 1 || y < py0 || y >= py0 + g.th || y >= height) continue;
+            for (int c = lane; c < g.tw; c += 32)
+                if (px0 + c < width)
+                    R.data[(long)(4 * kb + sub) * R.stride + px0 + c] = src[(y - py0 + kHalo) * g.pitch + c + kHalo];
+        }
+    }
+
+    // ---- CDEF on the deblocked tile
+    if (!s_any) {
+        // Nothing filtered (or CDEF off): the output is the deblocked tile.
+        for (int p = 0; p < a.num_planes; ++p) {
+            const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+            const DevPlane& d = a.dst[p];
+            const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+            const uint16_t* t = smem + a.plane_off[p];
+            for (int r = warp; r < g.th; r += kThreads / 32) {
+                const int y = py0 + r;
+                if (y >= d.height) break;
+                for (int c = lane; c < g.tw; c += 32)
+                    if (px0 + c < d.width) d.data[(long)y * d.stride + px0 + c] = t[(r + kHalo) * g.pitch + c + kHalo];
+            }
+        }
+        return;
+    }
+    // Samples outside the plane become the "unavailable" sentinel for CDEF.
+    for (int p = 0; p < a.num_planes; ++p) {
+        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        const DevPlane& d = a.dst[p];
+        const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+        if (px0 + g.tw + 2 <= d.width && py0 + g.th + 2 <= d.height && px0 >= 2 && py0 >= 2) continue;
+        uint16_t* t = smem + a.plane_off[p];
+        const int wr = g.th + 4, wc = g.tw + 4;
+        for (int i = tid; i < wr * wc; i += kThreads) {
+            const int r = i / wc, c = i - r * wc;
+            const int y = py0 - 2 + r, x = px0 - 2 + c;
+            if (y < 0 || x < 0 || y >= d.height || x >= d.width)
+                t[(r + kHalo - 2) * g.pitch + (c + kHalo - 2)] = (uint16_t)kSent;
+        }
+    }
+    __syncthreads();
+
+    // Direction search: warp w handles direction pair (w & 3) for blocks
+    // (w >> 2)*32 + lane (warp-uniform branches).
+    const int lpitch = 64 + 2 * kHalo;
+    {
+        const int pair = warp & 3, b = ((warp >> 2) << 5) + lane;
+        if (s_active[b]) {
+            const uint16_t* blk = smem + a.plane_off[0] + (kHalo + (b >> 3) * 8) * lpitch + kHalo + (b & 7) * 8;
+            int lo, hi;
+            dir_costs_pair(pair, blk, lpitch, a.shift, lo, hi);
+            s_cost[b][pair] = lo;
+            s_cost[b][pair + 4] = hi;
+        }
+    }
+    __syncthreads();
+    if (tid < 64 && s_active[tid]) {
+        const int b = tid;
+        int dir;
+        uint32_t var;
+        best_direction(s_cost[b], dir, var);
+        bool bad = false;
+        int bad_plane = 0, bad_msg = 0;
+        for (int p = 0; p < a.num_planes; ++p) {
+            const bool chroma = p != 0;
+            int sp = 0, ss = 0;
+            if (index < 8) {
+                sp = chroma ? a.uv_pri[index] : a.y_pri[index];
+                ss = chroma ? a.uv_sec[index] : a.y_sec[index];
+            }
+            int primary = (sp << a.shift) & 0xFFFF;
+            const int secondary = (ss << a.shift) & 0xFFFF;
+            const int chosen = primary == 0 ? 0 : chroma ? chroma_direction(dir, a.ssx, a.ssy) : dir;
+            if (!chroma) primary = adjust_strength(primary, var);
+            const int damping = (a.damping + a.shift - (chroma ? 1 : 0)) & 0xFF;
+            if (!bad && (index >= 8 || damping > 12 || primary > (15 << a.shift) || secondary > (4 << a.shift))) {
+                bad = true;
+                bad_plane = p;
+                bad_msg = index >= 8 ? VACO_AV1_MSG_CDEF_STRENGTH_INDEX : VACO_AV1_MSG_CDEF_BLOCK_PARAMS;
+            }
+            const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+            s_pair[p][b] = make_pair_block(chosen, primary, secondary, min(damping, 12), a.shift, g.pitch);
+        }
+        if (bad) {
+            const int r = mi_r0 + (b >> 3) * 2, c = mi_c0 + (b & 7) * 2;
+            report_error(a.status, STAGE_CDEF, ((unsigned long long)r * a.mi_cols + c) * 4 + 1 + bad_plane, bad_msg);
+        }
+    }
+    __syncthreads();
+
+    // Filtering: pixel pairs (two 16-bit lanes per register), one warp per
+    // block row, lanes across the tile width.
+    for (int p = 0; p < a.num_planes; ++p) {
+        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        const DevPlane& d = a.dst[p];
+        const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+        const bool edge = px0 < 2 || py0 < 2 || px0 + g.tw + 2 > d.width || py0 + g.th + 2 > d.height;
+        const uint16_t* tp = smem + a.plane_off[p];
+        if (g.pitch == 96 && g.th == 64) {
+            filter_pairs<96, 8, 1>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
+        } else if (g.pitch == 64 && g.th == 32) {
+            filter_pairs<64, 4, 2>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
+        } else {
+            filter_pairs<64, 8, 2>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
+    DbCdefArgs a;
+    const int np = L.info.monochrome ? 1 : 3;
+    bool vec = true;
+    size_t off = 0;
+    for (int p = 0; p < 3; ++p) {
+        a.src[p] = DevPlaneC{L.src.planes[p], L.src.width[p], L.src.height[p], L.src.stride[p]};
+        a.dst[p] = DevPlane{L.dst.planes[p], L.dst.width[p], L.dst.height[p], L.dst.stride[p]};
+        a.pre_rows[p] = L.pre_rows[p];
+        a.plane_off[p] = off;
+        if (p < np) {
+            vec = vec && (L.src.stride[p] % 8 == 0) && ((uintptr_t)L.src.planes[p] % 16 == 0);
+            const int sx = p ? L.info.subsampling_x : 0, sy = p ? L.info.subsampling_y : 0;
+            off += (size_t)((64 >> sx) + 2 * kHalo) * ((64 >> sy) + 2 * kHalo);
+        }
+    }
+    a.num_planes = np;
+    a.ssx = np > 1 ? L.info.subsampling_x : 0;
+    a.ssy = np > 1 ? L.info.subsampling_y : 0;
+    a.bit_depth = L.info.bit_depth;
+    a.shift = L.info.bit_depth - 8;
+    a.mi_rows = L.info.mi_rows;
+    a.mi_cols = L.info.mi_cols;
+    a.coded_width = L.info.coded_width;
+    a.coded_height = L.info.coded_height;
+    a.tx_luma = L.tx_luma;
+    a.tx_chroma = L.tx_chroma;
+    a.lvl_map = L.lvl_map;
+    for (int k = 0; k < 4; ++k) a.levels[k] = L.deblock.levels[k];
+    a.sharpness = L.deblock.sharpness;
+    a.deblock_on = !(L.deblock.levels[0] == 0 && L.deblock.levels[1] == 0);
+    bool all_zero = true;
+    for (int k = 0; k < 8; ++k)
+        all_zero = all_zero && L.cdef.y_primary[k] == 0 && L.cdef.y_secondary[k] == 0 && L.cdef.uv_primary[k] == 0 &&
+                   L.cdef.uv_secondary[k] == 0;
+    a.cdef_on = L.cdef.enabled && !all_zero && L.skip != nullptr;
+    a.skip = L.skip;
+    a.cdef_idx = L.cdef_idx;
+    a.cdef_stride = L.cdef_stride;
+    a.cdef_count = L.cdef_idx ? L.cdef_count : 0;
+    a.damping = L.cdef.damping;
+    for (int k = 0; k < 8; ++k) {
+        a.y_pri[k] = L.cdef.y_primary[k];
+        a.y_sec[k] = L.cdef.y_secondary[k];
+        a.uv_pri[k] = L.cdef.uv_primary[k];
+        a.uv_sec[k] = L.cdef.uv_secondary[k];
+    }
+    a.status = L.status;
+    a.vec_ok = vec;
+    const size_t smem = off * sizeof(uint16_t);
+    static unsigned long long attr_devices = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !(attr_devices & (1ull << dev))) {
+        cudaError_t e = cudaFuncSetAttribute(dbcdef_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_devices |= 1ull << dev;
+    }
+    dim3 grid(div_up(L.info.mi_cols, 16), div_up(L.info.mi_rows, 16));
+    dbcdef_kernel<<<grid, kThreads, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace vaco

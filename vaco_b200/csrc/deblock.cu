@@ -16,133 +16,20 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "deblock_core.cuh"
 #include "kernels.cuh"
 
 namespace vaco {
 
 namespace {
 
-struct Strength {
-    int limit, blimit, thresh;
-};
-
-// 7.14.4: limit / blimit / thresh from the level and sharpness.
-__device__ __forceinline__ Strength strength_of(int lvl, int sharpness) {
-    int shift = sharpness > 4 ? 2 : sharpness > 0 ? 1 : 0;
-    int limit = sharpness > 0 ? clampi(lvl >> shift, 1, 9 - sharpness) : max(1, lvl >> shift);
-    return Strength{limit, 2 * (lvl + 2) + limit, lvl >> 4};
-}
-
-// One line of samples across an edge; q0 at `q`, samples `step` apart.
-// nq / np: samples that exist on the q / p side inside the plane (reads past
-// them repeat the last one, writes past them are dropped).
-__device__ __forceinline__ void filter_line(uint16_t* q, long step, int nq, int np, int plane, int size,
-                                            const Strength& s, int bd) {
-    const int reach = size == 16 ? 7 : 4;
-    int Q[7], Pp[7];
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        if (k < reach) {
-            Q[k] = q[step * min(k, nq - 1)];
-            Pp[k] = q[-step * min(k + 1, np)];
-        } else {
-            Q[k] = Pp[k] = 0;
-        }
-    }
-    const int len = size == 4 ? 4 : plane != 0 ? 6 : size == 8 ? 8 : 16;
-    const int sh = bd - 8;
-    const int limit = s.limit << sh, blimit = s.blimit << sh, thresh = s.thresh << sh;
-    const bool hev = abs(Pp[1] - Pp[0]) > thresh || abs(Q[1] - Q[0]) > thresh;
-    bool mask = abs(Pp[1] - Pp[0]) > limit || abs(Q[1] - Q[0]) > limit ||
-                abs(Pp[0] - Q[0]) * 2 + abs(Pp[1] - Q[1]) / 2 > blimit;
-    if (len >= 6) mask = mask || abs(Pp[2] - Pp[1]) > limit || abs(Q[2] - Q[1]) > limit;
-    if (len >= 8) mask = mask || abs(Pp[3] - Pp[2]) > limit || abs(Q[3] - Q[2]) > limit;
-    if (mask) return;
-    const int one = 1 << sh;
-    bool flat = false, flat2 = false;
-    if (size >= 8) {
-        bool f = abs(Pp[1] - Pp[0]) > one || abs(Q[1] - Q[0]) > one || abs(Pp[2] - Pp[0]) > one ||
-                 abs(Q[2] - Q[0]) > one;
-        if (len >= 8) f = f || abs(Pp[3] - Pp[0]) > one || abs(Q[3] - Q[0]) > one;
-        flat = !f;
-    }
-    if (size >= 16) {
-        bool f = abs(Pp[6] - Pp[0]) > one || abs(Q[6] - Q[0]) > one || abs(Pp[5] - Pp[0]) > one ||
-                 abs(Q[5] - Q[0]) > one || abs(Pp[4] - Pp[0]) > one || abs(Q[4] - Q[0]) > one;
-        flat2 = !f;
-    }
-    auto put = [&](int k, int v) {
-        if (k >= 0 ? k < nq : -k <= np) q[step * k] = (uint16_t)v;
-    };
-    if (size == 4 || !flat) {
-        // 7.14.6.3 narrow filter
-        const int half = 0x80 << sh, lo = -(1 << (bd - 1)), hi = (1 << (bd - 1)) - 1;
-        const int ps1 = Pp[1] - half, ps0 = Pp[0] - half, qs0 = Q[0] - half, qs1 = Q[1] - half;
-        int f = hev ? clampi(ps1 - qs1, lo, hi) : 0;
-        f = clampi(f + 3 * (qs0 - ps0), lo, hi);
-        const int f1 = clampi(f + 4, lo, hi) >> 3;
-        const int f2 = clampi(f + 3, lo, hi) >> 3;
-        put(0, clampi(qs0 - f1, lo, hi) + half);
-        put(-1, clampi(ps0 + f2, lo, hi) + half);
-        if (!hev) {
-            const int f3 = (f1 + 1) >> 1;
-            put(1, clampi(qs1 - f3, lo, hi) + half);
-            put(-2, clampi(ps1 + f3, lo, hi) + half);
-        }
-        return;
-    }
-    // 7.14.6.4 wide filters: F[k] = q_k (k >= 0), p_{-k-1} (k < 0)
-    if (size == 8 || !flat2) {
-        if (plane == 0) {  // 8-tap, n = 3, center tap weight 2
-            const int p3 = Pp[3], p2 = Pp[2], p1 = Pp[1], p0 = Pp[0], q0 = Q[0], q1 = Q[1], q2 = Q[2], q3 = Q[3];
-            put(-3, (3 * p3 + 2 * p2 + p1 + p0 + q0 + 4) >> 3);
-            put(-2, (2 * p3 + p2 + 2 * p1 + p0 + q0 + q1 + 4) >> 3);
-            put(-1, (p3 + p2 + p1 + 2 * p0 + q0 + q1 + q2 + 4) >> 3);
-            put(0, (p2 + p1 + p0 + 2 * q0 + q1 + q2 + q3 + 4) >> 3);
-            put(1, (p1 + p0 + q0 + 2 * q1 + q2 + 2 * q3 + 4) >> 3);
-            put(2, (p0 + q0 + q1 + 2 * q2 + 3 * q3 + 4) >> 3);
-        } else {  // 6-tap chroma, n = 2, taps within |j| <= 1 weigh 2
-            const int p2 = Pp[2], p1 = Pp[1], p0 = Pp[0], q0 = Q[0], q1 = Q[1], q2 = Q[2];
-            put(-2, (3 * p2 + 2 * p1 + 2 * p0 + q0 + 4) >> 3);
-            put(-1, (p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3);
-            put(0, (p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3);
-            put(1, (p0 + 2 * q0 + 2 * q1 + 3 * q2 + 4) >> 3);
-        }
-        return;
-    }
-    // 14-tap, n = 6, log2 size 4
-    int F[14];
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        F[7 + k] = Q[k];
-        F[6 - k] = Pp[k];
-    }
-    int out[12];
-#pragma unroll
-    for (int i = -6; i < 6; ++i) {
-        int t = 0;
-#pragma unroll
-        for (int j = -6; j <= 6; ++j) {
-            int pos = min(max(i + j, -7), 6);
-            t += F[pos + 7] * ((j >= -1 && j <= 1) ? 2 : 1);
-        }
-        out[i + 6] = (t + 8) >> 4;
-    }
-#pragma unroll
-    for (int i = -6; i < 6; ++i) put(i, out[i + 6]);
-}
+using namespace dbk;
 
 struct PassArgs {
     DeblockLaunch L;
     int plane_list[3];
     int nplanes;
 };
-
-__device__ __forceinline__ int level_at(const DeblockLaunch& L, int plane, int pass, int row, int col) {
-    const int i = plane == 0 ? pass : plane + 1;
-    if (L.lvl_map) return L.lvl_map[((long)row * L.mi_cols + col) * 4 + i];
-    return L.levels[i];
-}
 
 // Pass 0: vertical edges.  x = edge index (plane column 4g), y = sample row.
 __global__ void deblock_vertical_kernel(PassArgs a) {

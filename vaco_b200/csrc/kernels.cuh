@@ -37,6 +37,11 @@ cudaError_t launch_superres(const SuperresPlane* planes, int count, int bit_dept
 // ---------------------------------------------------------------- restoration
 struct LrPlane {
     DevPlaneC before;
+    // When before_rows.data is set, the pre-CDEF picture is read from this
+    // compact buffer instead of `before`: 4 rows per stripe boundary k, rows
+    // (k*stripe - offset) - 2 .. +1 at indices 4k .. 4k+3 (as written by the
+    // fused deblock+CDEF kernel).
+    DevPlaneC before_rows;
     DevPlaneC after;
     DevPlane out;
     int width, height, unit_size, sub_y;
@@ -70,5 +75,28 @@ cudaError_t launch_deblock_prepare(const DevPlaneC* src, const DevPlane* dst, in
                                    const uint8_t* tx_luma, long n_luma, const uint8_t* tx_chroma, long n_chroma,
                                    const uint8_t* lvl_map, DeviceStatus* status, cudaStream_t stream);
 cudaError_t launch_deblock_passes(const DeblockLaunch& L, cudaStream_t stream);
+
+// ---------------------------------------------------------------- fused deblock + CDEF
+struct DbCdefLaunch {
+    vaco_av1_picture src;       // reconstruction (device)
+    vaco_av1_picture dst;       // CDEF output (device, same extents)
+    DevPlane pre_rows[3];       // compact stripe-boundary rows (data may be null)
+    vaco_av1_frame_info info;
+    const uint8_t* tx_luma;
+    const uint8_t* tx_chroma;
+    const uint8_t* lvl_map;
+    vaco_av1_deblock_params deblock;
+    const uint8_t* skip;
+    const int32_t* cdef_idx;
+    int cdef_stride, cdef_count;
+    vaco_av1_cdef_params cdef;
+    DeviceStatus* status;
+};
+cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream);
+// Rows in the compact boundary buffer of a plane of `height` rows.
+inline int pre_rows_count(int height, int sub_y) {
+    const int sh = 64 >> sub_y, off = 8 >> sub_y;
+    return 4 * ((height + off + 2) / sh + 1);
+}
 
 }  // namespace vaco

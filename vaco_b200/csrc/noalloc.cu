@@ -290,6 +290,7 @@ extern "C" int32_t vaco_av1_postfilter_frame_noalloc(void* stream, const vaco_av
             if (e != cudaSuccess) return fail(msg, VACO_AV1_DEVICE_ERROR, VACO_AV1_MSG_CUDA);
             LrPlane& p = lp[nlr++];
             p.before = DevPlaneC{before[k].data, before[k].width, before[k].height, before[k].stride};
+            p.before_rows = DevPlaneC{nullptr, 0, 0, 0};
             p.after = DevPlaneC{after[k].data, after[k].width, after[k].height, after[k].stride};
             p.out = DevPlane{J.dst.planes[k], w, h, J.dst.stride[k]};
             p.width = w;

@@ -10,13 +10,19 @@
 // min(unit, 64).  The CTA stages Source::get() of its tile plus a 3-sample
 // halo (the reach of the 7-tap Wiener filter and of a radius-2 box around a
 // radius-1 neighbourhood) in shared memory, so the stripe rule and the frame
-// clamps are applied once per staged sample instead of once per tap.
+// clamps are applied once per staged sample instead of once per tap.  Rows
+// are staged as aligned 16-byte vectors covering columns x0-8 .. x0+72.
 //   Wiener: the reference's 7x7 sum is separable sample-for-sample (the
 //           horizontal rounding/clip depends only on the source row), so it
 //           runs as a horizontal pass into an int16 buffer then a vertical pass.
 //   Self-guided: box sums per neighbour position are computed once per tile
 //           position (vaco recomputes them for every pixel that needs them),
-//           with a2 from a 256-entry table of ((z << 8) + z/2) / (z + 1).
+//           radius-specialised and unrolled, with a2 from a 256-entry table of
+//           ((z << 8) + z/2) / (z + 1).  The two passes run one after the
+//           other in the same shared buffers; each thread keeps its pixels'
+//           first-pass values in registers.
+// Thread mappings put consecutive lanes on consecutive columns, so shared
+// memory reads are conflict-free and global writes coalesce.
 #include <algorithm>
 
 #include "common.cuh"
@@ -27,11 +33,13 @@ namespace vaco {
 namespace {
 
 constexpr int kLrThreads = 256;
+constexpr int kWarps = kLrThreads / 32;
 constexpr int kMaxTile = 64;
-constexpr int kSPitch = kMaxTile + 8;                 // staged source pitch (>= C + 6)
-constexpr int kSRows = kMaxTile + 6;
-constexpr int kBoxPitch = kMaxTile + 2;
-constexpr int kBoxRows = kMaxTile + 2;
+constexpr int kSPitch = kMaxTile + 16;  // staged columns x0-8 .. x0+72
+constexpr int kSRows = kMaxTile + 6;    // staged rows y0-3 .. y0+67
+constexpr int kSOff = 8;                // staged column of x0
+constexpr int kBox = kMaxTile + 2;      // box positions y0-1 .. y0+64 (and x)
+constexpr int kPix = kMaxTile * kMaxTile / kLrThreads;  // pixels per thread (16)
 
 // Sgr_Params (radius, epsilon) per set and pass (restoration.rs:286-303).
 __constant__ int8_t c_sgr_r[16][2] = {{2, 1}, {2, 1}, {2, 1}, {2, 1}, {2, 1}, {2, 1}, {2, 1}, {2, 1},
@@ -49,25 +57,66 @@ struct LrArgs {
 };
 
 // Shared-memory layout (dynamic):
-//   S     kSRows x kSPitch uint16   staged Source::get values
-//   then either  H  kSRows x kMaxTile int16   (Wiener horizontal pass)
-//   or           A0,B0,A1,B1  kBoxRows x kBoxPitch int32 each (self-guided)
-//   a2 table     256 uint16
+//   S      kSRows x kSPitch uint16        staged Source::get values
+//   region either H  kSRows x kMaxTile int16   (Wiener horizontal pass)
+//          or     A  kBox x kBox uint16, B  kBox x kBox int32 (one self-guided pass)
+//   a2tab  256 uint16
 constexpr size_t kSBytes = sizeof(uint16_t) * kSRows * kSPitch;
-constexpr size_t kBoxBytes = sizeof(int32_t) * kBoxRows * kBoxPitch;
-constexpr size_t kLrSmem = kSBytes + 4 * kBoxBytes + 256 * sizeof(uint16_t);
+constexpr size_t kABytes = (sizeof(uint16_t) * kBox * kBox + 15) / 16 * 16;
+constexpr size_t kBBytes = sizeof(int32_t) * kBox * kBox;
+constexpr size_t kHBytes = sizeof(int16_t) * kSRows * kMaxTile;
+constexpr size_t kRegion = (kABytes + kBBytes) > kHBytes ? (kABytes + kBBytes) : kHBytes;
+constexpr size_t kLrSmem = kSBytes + kRegion + 256 * sizeof(uint16_t);
 
 __device__ __forceinline__ int round2i(int v, int s) { return s == 0 ? v : (v + (1 << (s - 1))) >> s; }
 
-__global__ void __launch_bounds__(kLrThreads) restoration_kernel(LrArgs a) {
+// Box sums around every position of one row band and the a2 / b terms of
+// box_ab (restoration.rs:314-339).
+template <int RAD>
+__device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_t* __restrict__ A,
+                                         int32_t* __restrict__ B, const uint16_t* __restrict__ a2tab, int R, int C,
+                                         int y_lo, bool odd_rows_only, int bd, unsigned scale) {
+    constexpr int n = (2 * RAD + 1) * (2 * RAD + 1);
+    constexpr unsigned recip = ((1 << 12) + n / 2) / n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rows = R + 2, cols = C + 2;
+    const int sh2 = 2 * (bd - 8), sh1 = bd - 8;
+    // First box row whose y (= y_lo - 1 + br) is odd, when only odd rows are used.
+    const int br0 = odd_rows_only ? ((y_lo - 1) & 1 ? 0 : 1) : 0;
+    const int rstep = odd_rows_only ? 2 : 1;
+    for (int br = br0 + warp * rstep; br < rows; br += kWarps * rstep) {
+        // staged row of box row br is br + 2 (box rows start at y0-1, staged at y0-3)
+        const uint16_t* srow = S + (br + 2 - RAD) * kSPitch + (kSOff - 1 - RAD);
+        for (int bc = lane; bc < cols; bc += 32) {
+            int sum = 0, sum_sq = 0;
+#pragma unroll
+            for (int dy = 0; dy <= 2 * RAD; ++dy)
+#pragma unroll
+                for (int dx = 0; dx <= 2 * RAD; ++dx) {
+                    int v = srow[dy * kSPitch + bc + dx];
+                    sum += v;
+                    sum_sq += v * v;
+                }
+            int aa = round2i(sum_sq, sh2);
+            int d = round2i(sum, sh1);
+            int p = max(aa * n - d * d, 0);
+            unsigned long long zz = ((unsigned long long)(unsigned)p * scale + (1u << 19)) >> 20;
+            int a2 = a2tab[zz > 255 ? 255 : (int)zz];
+            unsigned b = ((unsigned)(256 - a2) * (unsigned)sum * recip + (1u << 11)) >> 12;
+            A[br * kBox + bc] = (uint16_t)a2;
+            B[br * kBox + bc] = (int)b;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kLrThreads, 4) restoration_kernel(LrArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint16_t* S = reinterpret_cast<uint16_t*>(smem_raw);
-    int32_t* A0 = reinterpret_cast<int32_t*>(smem_raw + kSBytes);
-    int32_t* B0 = A0 + kBoxRows * kBoxPitch;
-    int32_t* A1 = B0 + kBoxRows * kBoxPitch;
-    int32_t* B1 = A1 + kBoxRows * kBoxPitch;
-    int16_t* H = reinterpret_cast<int16_t*>(A0);
-    uint16_t* a2tab = reinterpret_cast<uint16_t*>(smem_raw + kSBytes + 4 * kBoxBytes);
+    unsigned char* region = smem_raw + kSBytes;
+    int16_t* H = reinterpret_cast<int16_t*>(region);
+    uint16_t* A = reinterpret_cast<uint16_t*>(region);
+    int32_t* B = reinterpret_cast<int32_t*>(region + kABytes);
+    uint16_t* a2tab = reinterpret_cast<uint16_t*>(region + kRegion);
 
     int pl = 0;
     while (pl + 1 < a.count && (int)blockIdx.x >= a.tile_base[pl + 1]) ++pl;
@@ -80,8 +129,8 @@ __global__ void __launch_bounds__(kLrThreads) restoration_kernel(LrArgs a) {
     const int x_lo = tx * a.tile_w[pl];
     const int x_hi = min(x_lo + a.tile_w[pl], P.width);
     if (y_lo >= y_hi || x_lo >= x_hi) return;
-    const int R = y_hi - y_lo, Cw = x_hi - x_lo;
-    const int tid = threadIdx.x;
+    const int R = y_hi - y_lo, C = x_hi - x_lo;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     // Unit of this tile (unit_index, restoration.rs:124-133).
     const int urow = min((y_lo + off) / P.unit_size, P.unit_rows - 1);
@@ -90,30 +139,45 @@ __global__ void __launch_bounds__(kLrThreads) restoration_kernel(LrArgs a) {
     const int bd = a.bit_depth, maxv = (1 << bd) - 1;
 
     if (u.type != VACO_AV1_LR_WIENER && u.type != VACO_AV1_LR_SGRPROJ) {
-        for (int i = tid; i < R * Cw; i += kLrThreads) {
-            int yy = y_lo + i / Cw, xx = x_lo + i % Cw;
-            P.out.data[(long)yy * P.out.stride + xx] = P.after.data[(long)yy * P.after.stride + xx];
+        // RestorationUnit::None: the CDEF output, restoration.rs:194.
+        for (int k = warp; k < R; k += kWarps) {
+            const uint16_t* src = P.after.data + (long)(y_lo + k) * P.after.stride + x_lo;
+            uint16_t* dst = P.out.data + (long)(y_lo + k) * P.out.stride + x_lo;
+            for (int c = lane; c < C; c += 32) dst[c] = src[c];
         }
         return;
     }
 
-    // Stage Source::get (restoration.rs:233-244) for rows y_lo-3 .. y_hi+2,
-    // cols x_lo-3 .. x_hi+2.
+    // Stage Source::get (restoration.rs:233-244): rows y_lo-3 .. y_hi+2,
+    // columns x_lo-8 .. x_lo+72 as 10 aligned 8-sample vectors per row.
     const int stripe = (y_lo + off) / sh;
     const int s_start = stripe * sh - off, s_end = s_start + sh - 1;
-    const int srows = R + 6, scols = Cw + 6;
-    for (int i = tid; i < srows * scols; i += kLrThreads) {
-        int r = i / scols, c = i - r * scols;
-        int x = clampi(x_lo - 3 + c, 0, P.width - 1);
-        int y = clampi(y_lo - 3 + r, 0, P.height - 1);
-        int v;
-        if (y < s_start)
-            v = __ldg(P.before.data + (long)max(y, s_start - 2) * P.before.stride + x);
-        else if (y > s_end)
-            v = __ldg(P.before.data + (long)min(y, s_end + 2) * P.before.stride + x);
-        else
-            v = __ldg(P.after.data + (long)y * P.after.stride + x);
-        S[r * kSPitch + c] = (uint16_t)v;
+    const int srows = R + 6;
+    const bool compact = P.before_rows.data != nullptr;
+    const DevPlaneC& BP = compact ? P.before_rows : P.before;
+    const bool vec_ok = ((BP.stride | P.after.stride) & 7) == 0 &&
+                        ((reinterpret_cast<uintptr_t>(BP.data) | reinterpret_cast<uintptr_t>(P.after.data)) & 15) == 0;
+    for (int i = tid; i < srows * (kSPitch / 8); i += kLrThreads) {
+        const int r = i / (kSPitch / 8), v = i - r * (kSPitch / 8);
+        const int y = clampi(y_lo - 3 + r, 0, P.height - 1);
+        const uint16_t* row;
+        if (y < s_start) {
+            const int yy = max(y, s_start - 2);
+            row = BP.data + (long)(compact ? 4 * stripe + (yy - (s_start - 2)) : yy) * BP.stride;
+        } else if (y > s_end) {
+            const int yy = min(y, s_end + 2);
+            row = BP.data + (long)(compact ? 4 * (stripe + 1) + 2 + (yy - (s_end + 1)) : yy) * BP.stride;
+        } else {
+            row = P.after.data + (long)y * P.after.stride;
+        }
+        const int x = x_lo - kSOff + 8 * v;
+        uint16_t* d = S + r * kSPitch + 8 * v;
+        if (vec_ok && x >= 0 && x + 8 <= P.width) {
+            *reinterpret_cast<uint4*>(d) = __ldg(reinterpret_cast<const uint4*>(row + x));
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) d[k] = __ldg(row + clampi(x + k, 0, P.width - 1));
+        }
     }
     __syncthreads();
 
@@ -129,22 +193,24 @@ __global__ void __launch_bounds__(kLrThreads) restoration_kernel(LrArgs a) {
             int a1 = u.vertical[0], b1 = u.vertical[1], c1 = u.vertical[2];
             vv[0] = vv[6] = a1; vv[1] = vv[5] = b1; vv[2] = vv[4] = c1; vv[3] = 128 - 2 * (a1 + b1 + c1);
         }
-        for (int i = tid; i < srows * Cw; i += kLrThreads) {
-            int r = i / Cw, c = i - r * Cw;
-            const uint16_t* s = S + r * kSPitch + c;
-            int h = 0;
+        for (int r = warp; r < srows; r += kWarps) {
+            const uint16_t* s = S + r * kSPitch + kSOff - 3;
+            for (int c = lane; c < C; c += 32) {
+                int h = 0;
 #pragma unroll
-            for (int t = 0; t < 7; ++t) h += hv[t] * s[t];
-            H[r * kMaxTile + c] = (int16_t)clampi(round2i(h, round_h), -offset, limit - offset);
+                for (int t = 0; t < 7; ++t) h += hv[t] * s[c + t];
+                H[r * kMaxTile + c] = (int16_t)clampi(round2i(h, round_h), -offset, limit - offset);
+            }
         }
         __syncthreads();
-        for (int i = tid; i < R * Cw; i += kLrThreads) {
-            int k = i / Cw, c = i - k * Cw;
-            int sum = 0;
+        for (int k = warp; k < R; k += kWarps) {
+            uint16_t* dst = P.out.data + (long)(y_lo + k) * P.out.stride + x_lo;
+            for (int c = lane; c < C; c += 32) {
+                int sum = 0;
 #pragma unroll
-            for (int t = 0; t < 7; ++t) sum += vv[t] * H[(k + t) * kMaxTile + c];
-            int v = clampi(round2i(sum, 14 - round_h), 0, maxv);
-            P.out.data[(long)(y_lo + k) * P.out.stride + x_lo + c] = (uint16_t)v;
+                for (int t = 0; t < 7; ++t) sum += vv[t] * H[(k + t) * kMaxTile + c];
+                dst[c] = (uint16_t)clampi(round2i(sum, 14 - round_h), 0, maxv);
+            }
         }
         return;
     }
@@ -155,75 +221,63 @@ __global__ void __launch_bounds__(kLrThreads) restoration_kernel(LrArgs a) {
     const int e0 = c_sgr_e[set][0], e1 = c_sgr_e[set][1];
     for (int z = tid; z < 256; z += kLrThreads)
         a2tab[z] = (uint16_t)(z >= 255 ? 256 : z == 0 ? 1 : ((z << 8) + z / 2) / (z + 1));
-    const int brow = R + 2, bcol = Cw + 2;  // box positions: y_lo-1.., x_lo-1..
-    for (int pass = 0; pass < 2; ++pass) {
-        const int rad = pass ? r1 : r0;
-        if (rad == 0) continue;
-        const int eps = pass ? e1 : e0;
-        const int n = (2 * rad + 1) * (2 * rad + 1);
-        const int n2e = n * n * eps;
-        const unsigned scale = (unsigned)(((1 << 20) + n2e / 2) / n2e);
-        const unsigned recip = (unsigned)(((1 << 12) + n / 2) / n);
-        int32_t* Ab = pass ? A1 : A0;
-        int32_t* Bb = pass ? B1 : B0;
-        __syncthreads();  // a2tab ready
-        for (int i = tid; i < brow * bcol; i += kLrThreads) {
-            int br = i / bcol, bc = i - br * bcol;
-            int y = y_lo - 1 + br;
-            if (pass == 0 && (y & 1) == 0) continue;  // first pass reads odd rows only
-            int sum = 0, sum_sq = 0;
-            const uint16_t* s = S + (br + 2 - rad) * kSPitch + (bc + 2 - rad);
-            for (int dy = 0; dy <= 2 * rad; ++dy)
-                for (int dx = 0; dx <= 2 * rad; ++dx) {
-                    int v = s[dy * kSPitch + dx];
-                    sum += v;
-                    sum_sq += v * v;
+    // Pixel (k, c) of this thread: k = warp + 8*j, c = lane + 32*q.
+    int first[kPix];
+    if (r0 != 0) {
+        const int n2e = 25 * 25 * e0;
+        __syncthreads();  // a2tab
+        box_pass<2>(S, A, B, a2tab, R, C, y_lo, true, bd, (unsigned)(((1 << 20) + n2e / 2) / n2e));
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kPix / 2; ++j)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int k = warp + kWarps * j, c = lane + 32 * q;
+                if (k >= R || c >= C) continue;
+                const int y = y_lo + k;
+                const int orig = S[(k + 3) * kSPitch + kSOff + c];
+                const int bi = (k + 1) * kBox + (c + 1);
+                if (y & 1) {  // weights 6 (centre) / 5 on the row itself, shift 4
+                    int aa = 6 * A[bi] + 5 * (A[bi - 1] + A[bi + 1]);
+                    int bb = 6 * B[bi] + 5 * (B[bi - 1] + B[bi + 1]);
+                    first[j * 2 + q] = round2i(aa * orig + bb, 8);
+                } else {      // the odd rows above and below, shift 5
+                    const int up = bi - kBox, dn = bi + kBox;
+                    int aa = 6 * (A[up] + A[dn]) + 5 * (A[up - 1] + A[up + 1] + A[dn - 1] + A[dn + 1]);
+                    int bb = 6 * (B[up] + B[dn]) + 5 * (B[up - 1] + B[up + 1] + B[dn - 1] + B[dn + 1]);
+                    first[j * 2 + q] = round2i(aa * orig + bb, 9);
                 }
-            int aa = round2i(sum_sq, 2 * (bd - 8));
-            int d = round2i(sum, bd - 8);
-            int p = max(aa * n - d * d, 0);
-            unsigned long long zz = ((unsigned long long)(unsigned)p * scale + (1u << 19)) >> 20;
-            int z = zz > 255 ? 255 : (int)zz;
-            int a2 = a2tab[z];
-            unsigned b = ((unsigned)(256 - a2) * (unsigned)sum * recip + (1u << 11)) >> 12;
-            Ab[br * kBoxPitch + bc] = a2;
-            Bb[br * kBoxPitch + bc] = (int)b;
-        }
+            }
     }
-    __syncthreads();
+    if (r1 != 0) {
+        const int n2e = 9 * 9 * e1;
+        __syncthreads();  // a2tab, and pass-0 readers of A/B are done
+        box_pass<1>(S, A, B, a2tab, R, C, y_lo, false, bd, (unsigned)(((1 << 20) + n2e / 2) / n2e));
+        __syncthreads();
+    }
     const int w0 = u.xqd[0], w1 = u.xqd[1];
-    for (int i = tid; i < R * Cw; i += kLrThreads) {
-        int k = i / Cw, c = i - k * Cw;
-        int y = y_lo + k;
-        int orig = S[(k + 3) * kSPitch + c + 3];
-        const int bi = (k + 1) * kBoxPitch + (c + 1);  // box index of (x, y)
-        int first, second;
-        if (r0 == 0) {
-            first = orig << 4;
-        } else if (y & 1) {
-            int aa = 6 * A0[bi] + 5 * (A0[bi - 1] + A0[bi + 1]);
-            int bb = 6 * B0[bi] + 5 * (B0[bi - 1] + B0[bi + 1]);
-            first = round2i(aa * orig + bb, 8);
-        } else {
-            int up = bi - kBoxPitch, dn = bi + kBoxPitch;
-            int aa = 6 * (A0[up] + A0[dn]) + 5 * (A0[up - 1] + A0[up + 1] + A0[dn - 1] + A0[dn + 1]);
-            int bb = 6 * (B0[up] + B0[dn]) + 5 * (B0[up - 1] + B0[up + 1] + B0[dn - 1] + B0[dn + 1]);
-            first = round2i(aa * orig + bb, 9);
+#pragma unroll
+    for (int j = 0; j < kPix / 2; ++j)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int k = warp + kWarps * j, c = lane + 32 * q;
+            if (k >= R || c >= C) continue;
+            const int orig = S[(k + 3) * kSPitch + kSOff + c];
+            const int f0 = r0 ? first[j * 2 + q] : orig << 4;
+            int f1 = orig << 4;
+            if (r1) {
+                const int bi = (k + 1) * kBox + (c + 1), up = bi - kBox, dn = bi + kBox;
+                int aa = 4 * (A[bi] + A[bi - 1] + A[bi + 1] + A[up] + A[dn]) +
+                         3 * (A[up - 1] + A[up + 1] + A[dn - 1] + A[dn + 1]);
+                int bb = 4 * (B[bi] + B[bi - 1] + B[bi + 1] + B[up] + B[dn]) +
+                         3 * (B[up - 1] + B[up + 1] + B[dn - 1] + B[dn + 1]);
+                f1 = round2i(aa * orig + bb, 9);
+            }
+            int v = round2i(w0 * f0 + w1 * (orig << 4) + (128 - w0 - w1) * f1, 11);
+            P.out.data[(long)(y_lo + k) * P.out.stride + x_lo + c] = (uint16_t)clampi(v, 0, maxv);
         }
-        if (r1 == 0) {
-            second = orig << 4;
-        } else {
-            int up = bi - kBoxPitch, dn = bi + kBoxPitch;
-            int aa = 4 * (A1[bi] + A1[bi - 1] + A1[bi + 1] + A1[up] + A1[dn]) +
-                     3 * (A1[up - 1] + A1[up + 1] + A1[dn - 1] + A1[dn + 1]);
-            int bb = 4 * (B1[bi] + B1[bi - 1] + B1[bi + 1] + B1[up] + B1[dn]) +
-                     3 * (B1[up - 1] + B1[up + 1] + B1[dn - 1] + B1[dn + 1]);
-            second = round2i(aa * orig + bb, 9);
-        }
-        int v = round2i(w0 * first + w1 * (orig << 4) + (128 - w0 - w1) * second, 11);
-        P.out.data[(long)y * P.out.stride + x_lo + c] = (uint16_t)clampi(v, 0, maxv);
-    }
 }
+
 
 __global__ void lr_unit_check_kernel(const vaco_av1_lr_unit* units, int n, DeviceStatus* st) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
