@@ -370,6 +370,56 @@ def run_gpu(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def run_batch(args, world, rank, local):
+    """Config 3: 64 frames of mixed sizes (16 each of 640x360 8-bit, 1280x720
+    8-bit, 1920x1080 10-bit, 3840x2160 10-bit), independently seeded, through
+    vaco_av1_postfilter_batch_dev (persistent per-stage kernels over a device
+    tile queue, CUDA-graph replay, tuned launch shape)."""
+    import torch
+
+    from vaco_b200 import autotune
+    from vaco_b200.gpu import Context, DeviceFrame
+
+    torch.cuda.set_device(local)
+    frames = []
+    for wl, count in synth.BATCH_MIX:
+        for i in range(count):
+            frames.append(synth.make_frame(wl, synth.seed_for(3, 1000 * rank + len(frames))))
+    ctx = Context(local)
+    tuning = autotune.load_tuning()
+    ctx.set_tuning(**tuning)
+    devs = [DeviceFrame(f, local) for f in frames]
+    stream = torch.cuda.current_stream(local)
+    jobs = ctx.batch_jobs(devs)
+    for _ in range(args.warmup):
+        st, _ = ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs)
+        assert all(s == 0 for s in st)
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    px = sum(f.output_pixels for f in frames)
+    req = sum(sum(frame_bytes(f)) for f in frames)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    if rank == 0:
+        print(json.dumps({
+            "metric": "AV1 post-filter Mpixel/s, batched mixed-resolution frames", "mode": "batch",
+            "value": round(px / (ms / 1e3) / 1e6, 1), "unit": "Mpixel/s", "ms_per_batch": round(ms, 4),
+            "frames_per_batch": len(frames), "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": "batch_mix_64", "mix": [[w.name, c] for w, c in synth.BATCH_MIX], "tuning": tuning},
+            "hbm_roofline": {"required_bytes_per_batch": int(req), "achieved_gbs": round(req / (ms / 1e3) / 1e9, 1),
+                             "peak": hbm, "frac": round(req / (ms / 1e3) / 1e9 / hbm, 4)},
+            "gpu_launches_per_batch": (ctx.launches - launches0) / max(1, args.steps),
+        }), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,11 +428,20 @@ def main():
     ap.add_argument("--impl", default="vaco_b200", choices=["vaco_b200", "reference"])
     ap.add_argument("--workload", default="chain_4k_10bit", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--mode", default="headline", choices=["headline", "batch", "serve"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.mode == "batch":
+        run_batch(args, world, rank, local)
+        return
+    if args.mode == "serve":
+        from vaco_b200 import serve
+
+        serve.bench_main(args, world, rank, local)
         return
     run_gpu(args, world, rank, local)
 

@@ -340,6 +340,32 @@ VACO_AV1_API int32_t vaco_av1_postfilter_frame_dev(vaco_av1_ctx* ctx, void* stre
 VACO_AV1_API int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job,
                                        int32_t* msg);
 
+/* ---------------------------------------------------------------- batched form */
+
+/* Launch-shape knobs for the batched form (no counterpart in vaco).  The
+ * values in tuned/ are picked by vaco_b200.autotune on the target GPU. */
+typedef struct vaco_av1_tuning {
+    int32_t dbcdef_ctas_per_sm;  /* persistent CTAs per SM, deblock+CDEF kernel (1..4) */
+    int32_t lr_ctas_per_sm;      /* persistent CTAs per SM, restoration kernel (1..4) */
+    int32_t use_graphs;          /* capture each batch composition once as a CUDA graph */
+    int32_t largest_first;       /* queue the largest frames' tiles first */
+} vaco_av1_tuning;
+
+VACO_AV1_API int32_t vaco_av1_ctx_set_tuning(vaco_av1_ctx* ctx, const vaco_av1_tuning* tuning);
+VACO_AV1_API int32_t vaco_av1_ctx_get_tuning(const vaco_av1_ctx* ctx, vaco_av1_tuning* tuning);
+
+/* The chain over `n` frames of any sizes and bit depths in one launch set
+ * (no counterpart in vaco, which filters one frame per decode_frame call,
+ * src/decode.rs:553-559).  Pointers in `jobs` are device pointers.
+ * Deblock+CDEF and restoration each run as one persistent kernel whose CTAs
+ * take superblock tiles of all frames from a device-side queue; every frame
+ * keeps its own status word.  statuses[i] / msgs[i] (both optional) receive
+ * frame i's result; the return value is VACO_AV1_OK when every frame
+ * succeeded, else the status of the first failing frame.  Synchronizes
+ * `stream` once for the whole batch. */
+VACO_AV1_API int32_t vaco_av1_postfilter_batch_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_frame_job* jobs,
+                                                   int32_t n, int32_t* statuses, int32_t* msgs);
+
 /* The whole chain for callers that cannot call cudaMalloc.  No counterpart in
  * vaco (vaco allocates every intermediate picture through its Budget).
  *

@@ -943,6 +943,7 @@ extern "C" int vo_sizeof(const char* name) {
         {"vaco_av1_lr_plane_config", (int)sizeof(vaco_av1_lr_plane_config)},
         {"vaco_av1_deblock_params", (int)sizeof(vaco_av1_deblock_params)},
         {"vaco_av1_frame_job", (int)sizeof(vaco_av1_frame_job)},
+        {"vaco_av1_tuning", (int)sizeof(vaco_av1_tuning)},
     };
     for (const Entry& e : kSizes)
         if (std::strcmp(e.n, name) == 0) return e.s;

@@ -1,0 +1,67 @@
+"""The batched form: many frames of different sizes and bit depths in one
+launch set (persistent per-stage kernels over a device tile queue, optionally
+replayed from a CUDA graph) give, frame by frame, exactly the single-frame
+results and the oracle's."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from vaco_b200 import abi, synth
+from vaco_b200.gpu import DeviceFrame
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_frames(seed0, small=True):
+    geoms = [(200, 136, 10, None), (328, 200, 10, 400), (64, 64, 8, None), (520, 264, 12, None),
+             (120, 72, 8, 136), (1280, 720, 8, None)]
+    if not small:
+        geoms.append((1920, 1080, 10, None))
+    return [synth.make_small(seed0 + i, w, h, bd, upscaled_width=up, sharpness=None, with_lvl_map=i % 2 == 1)
+            for i, (w, h, bd, up) in enumerate(geoms)]
+
+
+@pytest.mark.parametrize("graphs", [0, 1])
+@pytest.mark.parametrize("largest_first", [0, 1])
+def test_batch_matches_oracle_frame_by_frame(ctx, graphs, largest_first, oracle_threads):
+    ctx.set_tuning(use_graphs=graphs, largest_first=largest_first)
+    frames = mixed_frames(100, small=False)
+    devs = [DeviceFrame(f) for f in frames]
+    stream = torch.cuda.current_stream().cuda_stream
+    st, ms = ctx.postfilter_batch_dev(devs, stream=stream)
+    assert st == [0] * len(frames) and ms == [0] * len(frames)
+    for f, d in zip(frames, devs):
+        want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+        assert m == 0
+        for g, w in zip(d.outputs_numpy(), want):
+            np.testing.assert_array_equal(g, w)
+
+
+def test_batch_graph_replay_with_new_data(ctx, oracle_threads):
+    ctx.set_tuning(use_graphs=1)
+    stream = torch.cuda.current_stream().cuda_stream
+    for seed0 in (200, 300, 400):  # same composition, different frames: one capture, two replays
+        frames = mixed_frames(seed0)
+        devs = [DeviceFrame(f) for f in frames]
+        st, _ = ctx.postfilter_batch_dev(devs, stream=stream)
+        assert st == [0] * len(frames)
+        for f, d in zip(frames, devs):
+            want, _ = oracle.postfilter_frame(f, threads=oracle_threads)
+            for g, w in zip(d.outputs_numpy(), want):
+                np.testing.assert_array_equal(g, w)
+
+
+def test_batch_reports_errors_per_frame(ctx):
+    frames = mixed_frames(500)
+    frames[1].planes[0][3, 3] = 60000          # bad sample: deblocking check
+    frames[3].lr_units[1][0] = (abi.LR_SGRPROJ, 0, (0, 0, 0), (0, 0, 0), (40, 0))  # bad coefficient in plane U
+    devs = [DeviceFrame(f) for f in frames]
+    st, ms = ctx.postfilter_batch_dev(devs, stream=torch.cuda.current_stream().cuda_stream)
+    assert st[1] == abi.INVALID_DATA and ms[1] == abi.MSG["DB_SAMPLE"]
+    assert st[3] == abi.INVALID_DATA and ms[3] == abi.MSG["LR_COEFFICIENT"]
+    for i in (0, 2, 4, 5):
+        assert st[i] == abi.OK
+        want, _ = oracle.postfilter_frame(frames[i])
+        for g, w in zip(devs[i].outputs_numpy(), want):
+            np.testing.assert_array_equal(g, w)

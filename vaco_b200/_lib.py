@@ -38,6 +38,9 @@ SIGNATURES = [
     ("vaco_av1_deblock_picture_host", _i32, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _pi32]),
     ("vaco_av1_postfilter_frame_dev", _i32, [_vp, _vp, _vp, _pi32]),
     ("vaco_av1_postfilter_frame_host", _i32, [_vp, _vp, _pi32]),
+    ("vaco_av1_ctx_set_tuning", _i32, [_vp, _vp]),
+    ("vaco_av1_ctx_get_tuning", _i32, [_vp, _vp]),
+    ("vaco_av1_postfilter_batch_dev", _i32, [_vp, _vp, _vp, _i32, _vp, _vp]),
     ("vaco_av1_postfilter_frame_noalloc", _i32, [_vp, _vp, _pi32]),
 ]
 

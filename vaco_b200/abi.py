@@ -150,6 +150,15 @@ class FrameJob(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [
+        ("dbcdef_ctas_per_sm", C.c_int32),
+        ("lr_ctas_per_sm", C.c_int32),
+        ("use_graphs", C.c_int32),
+        ("largest_first", C.c_int32),
+    ]
+
+
 # numpy structured dtype with the vaco_av1_lr_unit layout (20 bytes)
 def lr_unit_dtype():
     import numpy as np
@@ -178,4 +187,5 @@ STRUCT_SIZES = {
     "vaco_av1_lr_plane_config": C.sizeof(LrPlaneConfig),
     "vaco_av1_deblock_params": C.sizeof(DeblockParams),
     "vaco_av1_frame_job": C.sizeof(FrameJob),
+    "vaco_av1_tuning": C.sizeof(Tuning),
 }

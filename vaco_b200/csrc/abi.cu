@@ -11,6 +11,7 @@
 #include <new>
 
 #include "common.cuh"
+#include "ctx.cuh"
 #include "kernels.cuh"
 
 using namespace vaco;
@@ -53,69 +54,8 @@ unsigned long long lr_position(int plane, unsigned check, unsigned long long ind
 
 bool bd_valid(int bd) { return bd == 8 || bd == 10 || bd == 12; }
 
-size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 }  // namespace
-
-struct vaco_av1_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    DeviceStatus* status = nullptr;           // device
-    unsigned long long* status_host = nullptr;  // pinned
-    int last_cuda_error = 0;
-    uint64_t launches = 0;
-    // stage timing (vaco_av1_ctx_set_stage_timing)
-    bool timing = false;
-    bool marks_pending = false;
-    cudaEvent_t marks[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    double stage_ms[4] = {0, 0, 0, 0};
-    uint64_t timed_frames = 0;
-
-    void mark(int i, cudaStream_t s) {
-        if (timing && marks[i]) {
-            cudaEventRecord(marks[i], s);
-            if (i == 4) marks_pending = true;
-        }
-    }
-    // Called after the stream has been synchronized.
-    void collect_marks() {
-        if (!marks_pending) return;
-        marks_pending = false;
-        for (int i = 0; i < 4; ++i) {
-            float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, marks[i], marks[i + 1]) == cudaSuccess) stage_ms[i] += ms;
-        }
-        ++timed_frames;
-    }
-    struct Buf {
-        void* p = nullptr;
-        size_t n = 0;
-    };
-    Buf bufs[24];
-
-    void* scratch(int slot, size_t bytes) {
-        Buf& b = bufs[slot];
-        if (b.n >= bytes && b.p) return b.p;
-        if (b.p) cudaFree(b.p);
-        b.p = nullptr;
-        b.n = 0;
-        size_t n = align_up(bytes < 256 ? 256 : bytes, 256);
-        if (cudaMalloc(&b.p, n) != cudaSuccess) return nullptr;
-        b.n = n;
-        return b.p;
-    }
-};
-
-// Scratch slots
-enum Slot {
-    S_PRE0 = 0, S_PRE1, S_PRE2,       // deblocked (pre-CDEF) planes
-    S_CDEF0, S_CDEF1, S_CDEF2,        // CDEF output planes
-    S_UPRE0, S_UPRE1, S_UPRE2,        // upscaled pre-CDEF planes
-    S_UCDEF0, S_UCDEF1, S_UCDEF2,     // upscaled CDEF planes
-    S_H_IN0, S_H_IN1, S_H_IN2,        // host-entry staging (inputs)
-    S_H_OUT0, S_H_OUT1, S_H_OUT2,     // host-entry staging (outputs)
-    S_H_SIDE0, S_H_SIDE1, S_H_SIDE2, S_H_SIDE3, S_H_SIDE4, S_H_SIDE5,
-};
 
 namespace {
 
@@ -375,6 +315,9 @@ void vaco_av1_ctx_destroy(vaco_av1_ctx* ctx) {
     if (ctx->status_host) cudaFreeHost(ctx->status_host);
     for (auto& ev : ctx->marks)
         if (ev) cudaEventDestroy(ev);
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
+    if (ctx->batch_table_host) cudaFreeHost(ctx->batch_table_host);
+    if (ctx->batch_status_host) cudaFreeHost(ctx->batch_status_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -621,7 +564,7 @@ int32_t vaco_av1_restore_plane_dev(vaco_av1_ctx* ctx, void* stream, const uint16
     cudaStream_t s = (cudaStream_t)stream;
     cudaSetDevice(ctx->device);
     cudaError_t e = reset_status(ctx, s);
-    if (e == cudaSuccess) e = launch_lr_unit_check(units, unit_count, ctx->status, s);
+    if (e == cudaSuccess) e = launch_lr_unit_check(units, unit_count, 0, ctx->status, s);
     const int maxv = (1 << config->bit_depth) - 1;
     if (e == cudaSuccess)
         e = launch_range_check(DevPlaneC{before, before_width, before_height, before_stride}, config->width,
@@ -647,6 +590,7 @@ int32_t vaco_av1_restore_plane_dev(vaco_av1_ctx* ctx, void* stream, const uint16
     p.units = units;
     p.unit_cols = cols;
     p.unit_rows = rows;
+    p.copy_only = 0;
     e = launch_restoration(&p, 1, config->bit_depth, s);
     ctx->launches++;
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
@@ -906,7 +850,7 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
                 hk = make_key(STAGE_LR, lr_position(k, LR_COUNT, 0), VACO_AV1_MSG_NULL_ARGUMENT);
                 break;
             }
-            e = launch_lr_unit_check(job->lr_units[k], job->lr_unit_count[k], ctx->status, s);
+            e = launch_lr_unit_check(job->lr_units[k], job->lr_unit_count[k], k, ctx->status, s);
             ctx->launches++;
             if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
             LrPlane& p = lp[nlr++];
@@ -921,6 +865,7 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
             p.units = job->lr_units[k];
             p.unit_cols = cols;
             p.unit_rows = rows;
+            p.copy_only = 0;
         }
         // Samples reaching restoration inside the chain were produced by the
         // deblocking / CDEF / superres kernels from range-checked input, so

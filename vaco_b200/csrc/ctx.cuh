@@ -1,0 +1,85 @@
+// ctx.cuh -- the vaco_av1_ctx object behind the C ABI (internal).
+#pragma once
+
+#include <map>
+#include <string>
+
+#include "common.cuh"
+
+namespace vaco {
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+}  // namespace vaco
+
+struct vaco_av1_ctx {
+    using size_t = ::size_t;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    vaco::DeviceStatus* status = nullptr;     // device
+    unsigned long long* status_host = nullptr;  // pinned
+    int last_cuda_error = 0;
+    uint64_t launches = 0;
+    // stage timing (vaco_av1_ctx_set_stage_timing)
+    bool timing = false;
+    bool marks_pending = false;
+    cudaEvent_t marks[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double stage_ms[4] = {0, 0, 0, 0};
+    uint64_t timed_frames = 0;
+
+    void mark(int i, cudaStream_t s) {
+        if (timing && marks[i]) {
+            cudaEventRecord(marks[i], s);
+            if (i == 4) marks_pending = true;
+        }
+    }
+    // Called after the stream has been synchronized.
+    void collect_marks() {
+        if (!marks_pending) return;
+        marks_pending = false;
+        for (int i = 0; i < 4; ++i) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, marks[i], marks[i + 1]) == cudaSuccess) stage_ms[i] += ms;
+        }
+        ++timed_frames;
+    }
+    struct Buf {
+        void* p = nullptr;
+        size_t n = 0;
+    };
+    Buf bufs[32];
+
+    // batched form (batch.cu)
+    vaco_av1_tuning tuning = {3, 4, 1, 1};
+    unsigned char* batch_table_host = nullptr;   // pinned staging of the per-batch tables
+    size_t batch_table_host_bytes = 0;
+    unsigned long long* batch_status_host = nullptr;  // pinned copy of the per-frame status words
+    size_t batch_status_host_count = 0;
+    std::map<std::string, cudaGraphExec_t> graphs;   // by batch composition (and scratch generation)
+    unsigned long long scratch_generation = 0;       // bumps whenever a scratch slot is reallocated
+    int sm_count = 0;
+
+    void* scratch(int slot, size_t bytes) {
+        Buf& b = bufs[slot];
+        if (b.n >= bytes && b.p) return b.p;
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.n = 0;
+        size_t n = vaco::align_up(bytes < 256 ? 256 : bytes, 256);
+        if (cudaMalloc(&b.p, n) != cudaSuccess) return nullptr;
+        b.n = n;
+        ++scratch_generation;
+        return b.p;
+    }
+};
+
+// Scratch slots
+enum Slot {
+    S_PRE0 = 0, S_PRE1, S_PRE2,       // deblocked (pre-CDEF) planes
+    S_CDEF0, S_CDEF1, S_CDEF2,        // CDEF output planes
+    S_UPRE0, S_UPRE1, S_UPRE2,        // upscaled pre-CDEF planes
+    S_UCDEF0, S_UCDEF1, S_UCDEF2,     // upscaled CDEF planes
+    S_H_IN0, S_H_IN1, S_H_IN2,        // host-entry staging (inputs)
+    S_H_OUT0, S_H_OUT1, S_H_OUT2,     // host-entry staging (outputs)
+    S_H_SIDE0, S_H_SIDE1, S_H_SIDE2, S_H_SIDE3, S_H_SIDE4, S_H_SIDE5,
+    S_BATCH_ARENA, S_BATCH_TABLE,      // batched form: intermediates, per-batch tables
+};
+

@@ -22,6 +22,7 @@
 // passes run one thread per edge line, in place; reads past the plane repeat
 // the edge sample and writes past it are dropped, as in deblock.cu.
 #include <algorithm>
+#include <cstring>
 
 #include "cdef_core.cuh"
 #include "common.cuh"
@@ -132,7 +133,10 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const DevPlane& 
     }
 }
 
-__global__ void __launch_bounds__(kThreads, 4) dbcdef_kernel(DbCdefArgs a) {
+// One 64x64 filter block (tile_x, tile_y) of one frame.  Every thread of the
+// CTA calls it; it ends with all threads past their last shared-memory use
+// only after the caller's next __syncthreads().
+__device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int tile_y) {
     extern __shared__ __align__(16) uint16_t smem[];
     __shared__ int s_cost[64][8];
     __shared__ PairBlock s_pair[3][64];
@@ -142,7 +146,7 @@ __global__ void __launch_bounds__(kThreads, 4) dbcdef_kernel(DbCdefArgs a) {
     __shared__ int s_any, s_bad;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int mi_r0 = blockIdx.y * 16, mi_c0 = blockIdx.x * 16;
+    const int mi_r0 = tile_y * 16, mi_c0 = tile_x * 16;
     const int x0 = mi_c0 * 4, y0 = mi_r0 * 4;
     const int maxv = (1 << a.bit_depth) - 1;
 
@@ -461,10 +465,53 @@ __global__ void __launch_bounds__(kThreads, 4) dbcdef_kernel(DbCdefArgs a) {
     }
 }
 
+__global__ void __launch_bounds__(kThreads, 4) dbcdef_kernel(DbCdefArgs a) { dbcdef_tile(a, blockIdx.x, blockIdx.y); }
+
+// Persistent form: CTAs take tiles of all frames of a batch from a device
+// queue (one atomic per tile), so frames of any size share one launch.
+__global__ void __launch_bounds__(kThreads, 4) dbcdef_batch_kernel(const DbCdefArgs* __restrict__ frames,
+                                                                   const int* __restrict__ tile_prefix, int n,
+                                                                   int* queue) {
+    __shared__ int s_tile, s_frame;
+    __shared__ DbCdefArgs s_args;
+    const int total = tile_prefix[n];
+    for (;;) {
+        __syncthreads();  // previous tile done with shared memory
+        if (threadIdx.x == 0) {
+            const int t = atomicAdd(queue, 1);
+            int lo = 0, hi = n - 1;  // last frame whose first tile is <= t
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (tile_prefix[mid] <= t) lo = mid; else hi = mid - 1;
+            }
+            s_tile = t;
+            s_frame = lo;
+        }
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= total) break;
+        const int f = s_frame;
+        {
+            const int words = (int)(sizeof(DbCdefArgs) / sizeof(int));
+            const int* src = reinterpret_cast<const int*>(frames + f);
+            int* dst = reinterpret_cast<int*>(&s_args);
+            for (int i = threadIdx.x; i < words; i += kThreads) dst[i] = src[i];
+        }
+        __syncthreads();
+        const int local = t - tile_prefix[f];
+        const int tiles_x = (s_args.mi_cols + 15) / 16;
+        dbcdef_tile(s_args, local % tiles_x, local / tiles_x);
+    }
+}
+
 }  // namespace
 
-cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
+size_t dbcdef_args_size() { return sizeof(DbCdefArgs); }
+
+// Kernel arguments of one frame; returns the dynamic shared memory it needs.
+size_t build_dbcdef_args(const DbCdefLaunch& L, void* out) {
     DbCdefArgs a;
+    memset(&a, 0, sizeof a);
     const int np = L.info.monochrome ? 1 : 3;
     bool vec = true;
     size_t off = 0;
@@ -512,17 +559,40 @@ cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
     }
     a.status = L.status;
     a.vec_ok = vec;
-    const size_t smem = off * sizeof(uint16_t);
+    memcpy(out, &a, sizeof a);
+    return off * sizeof(uint16_t);
+}
+
+cudaError_t dbcdef_kernel_attributes() {
     static unsigned long long attr_devices = 0;
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && !(attr_devices & (1ull << dev))) {
         cudaError_t e = cudaFuncSetAttribute(dbcdef_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(dbcdef_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
         if (e != cudaSuccess) return e;
         attr_devices |= 1ull << dev;
     }
+    return cudaSuccess;
+}
+
+cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
+    DbCdefArgs a;
+    const size_t smem = build_dbcdef_args(L, &a);
+    cudaError_t e = dbcdef_kernel_attributes();
+    if (e != cudaSuccess) return e;
     dim3 grid(div_up(L.info.mi_cols, 16), div_up(L.info.mi_rows, 16));
     dbcdef_kernel<<<grid, kThreads, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, size_t smem,
+                                int grid, cudaStream_t stream) {
+    cudaError_t e = dbcdef_kernel_attributes();
+    if (e != cudaSuccess) return e;
+    dbcdef_batch_kernel<<<grid, kThreads, smem, stream>>>(static_cast<const DbCdefArgs*>(dev_args), dev_prefix, n,
+                                                         dev_queue);
     return cudaGetLastError();
 }
 

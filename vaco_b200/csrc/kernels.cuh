@@ -47,12 +47,41 @@ struct LrPlane {
     int width, height, unit_size, sub_y;
     const vaco_av1_lr_unit* units;  // device
     int unit_cols, unit_rows;
+    int copy_only;                  // 1: output = `after` (frame-level restoration off for the plane)
 };
 // Restores up to 3 planes in one launch.  Units must have been validated.
 cudaError_t launch_restoration(const LrPlane* planes, int count, int bit_depth, cudaStream_t stream);
-// Reports VACO_AV1_MSG_LR_COEFFICIENT for the first invalid unit (key order:
-// before any sample error).
-cudaError_t launch_lr_unit_check(const vaco_av1_lr_unit* units, int n, DeviceStatus* status, cudaStream_t stream);
+// Batched form (see launch_dbcdef_batch): per-frame records of lr_args_size()
+// bytes built by build_lr_args (which returns the frame's tile count).
+size_t lr_args_size();
+int build_lr_args(const LrPlane* planes, int count, int bit_depth, void* out);
+cudaError_t launch_restoration_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, int grid,
+                                     cudaStream_t stream);
+// Reports VACO_AV1_MSG_LR_COEFFICIENT for invalid units of many unit arrays.
+// Shared-memory opt-ins of every kernel on the current device (idempotent);
+// call before stream capture.
+cudaError_t dbcdef_kernel_attributes();
+cudaError_t lr_kernel_attributes();
+inline cudaError_t kernel_attributes() {
+    cudaError_t e = dbcdef_kernel_attributes();
+    return e == cudaSuccess ? lr_kernel_attributes() : e;
+}
+struct UnitCheck {
+    const vaco_av1_lr_unit* units;
+    int count;
+    int plane;
+    DeviceStatus* status;
+};
+cudaError_t launch_lr_unit_check_batch(const UnitCheck* dev_checks, int n, int max_count, cudaStream_t stream);
+// Reports VACO_AV1_MSG_LR_COEFFICIENT for the first invalid unit of `plane`,
+// keyed after that plane's geometry/count checks and before its sample checks.
+cudaError_t launch_lr_unit_check(const vaco_av1_lr_unit* units, int n, int plane, DeviceStatus* status,
+                                 cudaStream_t stream);
+// LR status-key positions: plane, then the check restore_plane runs first.
+__host__ __device__ inline unsigned long long lr_key_position(int plane, unsigned check, unsigned long long index) {
+    return ((unsigned long long)plane << 44) | ((unsigned long long)check << 40) | index;
+}
+enum LrCheckOrder : unsigned { LRC_NO_UNIT_SIZE = 0, LRC_GEOMETRY = 1, LRC_COUNT = 2, LRC_COEFFICIENT = 3, LRC_SAMPLE = 4 };
 
 // ---------------------------------------------------------------- range checks / copies
 // Reports `msg` at (stage, `position`) if any sample of the w x h region exceeds max.
@@ -93,6 +122,14 @@ struct DbCdefLaunch {
     DeviceStatus* status;
 };
 cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream);
+// Batched form: `dev_args` holds n per-frame argument records (dbcdef_args_size()
+// bytes each, built by build_dbcdef_args), `dev_prefix` n+1 running tile
+// counts, `dev_queue` a zeroed counter.  `grid` persistent CTAs drain the queue.
+size_t dbcdef_args_size();
+size_t build_dbcdef_args(const DbCdefLaunch& L, void* out);  // returns dynamic smem bytes
+inline int dbcdef_tiles(const vaco_av1_frame_info& i) { return ((i.mi_cols + 15) / 16) * ((i.mi_rows + 15) / 16); }
+cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, size_t smem,
+                                int grid, cudaStream_t stream);
 // Rows in the compact boundary buffer of a plane of `height` rows.
 inline int pre_rows_count(int height, int sub_y) {
     const int sh = 64 >> sub_y, off = 8 >> sub_y;

@@ -286,7 +286,7 @@ extern "C" int32_t vaco_av1_postfilter_frame_noalloc(void* stream, const vaco_av
                                   J.lr_units[k] ? VACO_AV1_MSG_LR_UNIT_COUNT : VACO_AV1_MSG_NULL_ARGUMENT);
                 break;
             }
-            e = launch_lr_unit_check(J.lr_units[k], J.lr_unit_count[k], status, s);
+            e = launch_lr_unit_check(J.lr_units[k], J.lr_unit_count[k], k, status, s);
             if (e != cudaSuccess) return fail(msg, VACO_AV1_DEVICE_ERROR, VACO_AV1_MSG_CUDA);
             LrPlane& p = lp[nlr++];
             p.before = DevPlaneC{before[k].data, before[k].width, before[k].height, before[k].stride};
@@ -300,6 +300,7 @@ extern "C" int32_t vaco_av1_postfilter_frame_noalloc(void* stream, const vaco_av
             p.units = J.lr_units[k];
             p.unit_cols = cols;
             p.unit_rows = rows;
+            p.copy_only = 0;
         }
         if (host_key == kNoError && nlr > 0) {
             e = launch_restoration(lp, nlr, info.bit_depth, s);

@@ -24,6 +24,7 @@
 // Thread mappings put consecutive lanes on consecutive columns, so shared
 // memory reads are conflict-free and global writes coalesce.
 #include <algorithm>
+#include <cstring>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -109,7 +110,8 @@ __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_
     }
 }
 
-__global__ void __launch_bounds__(kLrThreads, 4) restoration_kernel(LrArgs a) {
+// One restoration tile: `block` indexes the tiles of all planes of `a`.
+__device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint16_t* S = reinterpret_cast<uint16_t*>(smem_raw);
     unsigned char* region = smem_raw + kSBytes;
@@ -119,9 +121,9 @@ __global__ void __launch_bounds__(kLrThreads, 4) restoration_kernel(LrArgs a) {
     uint16_t* a2tab = reinterpret_cast<uint16_t*>(region + kRegion);
 
     int pl = 0;
-    while (pl + 1 < a.count && (int)blockIdx.x >= a.tile_base[pl + 1]) ++pl;
+    while (pl + 1 < a.count && block >= a.tile_base[pl + 1]) ++pl;
     const LrPlane& P = a.p[pl];
-    const int local = blockIdx.x - a.tile_base[pl];
+    const int local = block - a.tile_base[pl];
     const int ty = local / a.tiles_x[pl], tx = local - ty * a.tiles_x[pl];
     const int off = a.off[pl], sh = a.stripe_h[pl];
     const int y_lo = max(ty * a.tile_h[pl] - off, 0);
@@ -135,10 +137,12 @@ __global__ void __launch_bounds__(kLrThreads, 4) restoration_kernel(LrArgs a) {
     // Unit of this tile (unit_index, restoration.rs:124-133).
     const int urow = min((y_lo + off) / P.unit_size, P.unit_rows - 1);
     const int ucol = min(x_lo / P.unit_size, P.unit_cols - 1);
-    const vaco_av1_lr_unit u = P.units[urow * P.unit_cols + ucol];
+    vaco_av1_lr_unit u;
+    if (P.copy_only) u.type = VACO_AV1_LR_NONE;
+    else u = P.units[urow * P.unit_cols + ucol];
     const int bd = a.bit_depth, maxv = (1 << bd) - 1;
 
-    if (u.type != VACO_AV1_LR_WIENER && u.type != VACO_AV1_LR_SGRPROJ) {
+    if (P.copy_only || (u.type != VACO_AV1_LR_WIENER && u.type != VACO_AV1_LR_SGRPROJ)) {
         // RestorationUnit::None: the CDEF output, restoration.rs:194.
         for (int k = warp; k < R; k += kWarps) {
             const uint16_t* src = P.after.data + (long)(y_lo + k) * P.after.stride + x_lo;
@@ -279,25 +283,70 @@ __global__ void __launch_bounds__(kLrThreads, 4) restoration_kernel(LrArgs a) {
 }
 
 
-__global__ void lr_unit_check_kernel(const vaco_av1_lr_unit* units, int n, DeviceStatus* st) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    vaco_av1_lr_unit u = units[i];
-    bool ok;
-    if (u.type == VACO_AV1_LR_NONE) {
-        ok = true;
-    } else if (u.type == VACO_AV1_LR_WIENER) {
+__global__ void __launch_bounds__(kLrThreads, 4) restoration_kernel(LrArgs a) { lr_tile(a, blockIdx.x); }
+
+// Persistent form over the tiles of all frames of a batch (see dbcdef.cu).
+__global__ void __launch_bounds__(kLrThreads, 4) restoration_batch_kernel(const LrArgs* __restrict__ frames,
+                                                                          const int* __restrict__ tile_prefix, int n,
+                                                                          int* queue) {
+    __shared__ int s_tile, s_frame;
+    __shared__ LrArgs s_args;
+    const int total = tile_prefix[n];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int t = atomicAdd(queue, 1);
+            int lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (tile_prefix[mid] <= t) lo = mid; else hi = mid - 1;
+            }
+            s_tile = t;
+            s_frame = lo;
+        }
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= total) break;
+        const int f = s_frame;
+        {
+            const int words = (int)(sizeof(LrArgs) / sizeof(int));
+            const int* src = reinterpret_cast<const int*>(frames + f);
+            int* dst = reinterpret_cast<int*>(&s_args);
+            for (int i = threadIdx.x; i < words; i += kLrThreads) dst[i] = src[i];
+        }
+        __syncthreads();
+        lr_tile(s_args, t - tile_prefix[f]);
+    }
+}
+
+__device__ __forceinline__ bool unit_ok(const vaco_av1_lr_unit& u) {
+    if (u.type == VACO_AV1_LR_NONE) return true;
+    if (u.type == VACO_AV1_LR_WIENER) {
         const int lo[3] = {-5, -23, -17}, hi[3] = {10, 8, 46};
-        ok = true;
+        bool ok = true;
         for (int k = 0; k < 3; ++k)
             ok = ok && u.vertical[k] >= lo[k] && u.vertical[k] <= hi[k] && u.horizontal[k] >= lo[k] &&
                  u.horizontal[k] <= hi[k];
-    } else if (u.type == VACO_AV1_LR_SGRPROJ) {
-        ok = u.set >= 0 && u.set < 16 && u.xqd[0] >= -96 && u.xqd[0] <= 31 && u.xqd[1] >= -32 && u.xqd[1] <= 95;
-    } else {
-        ok = false;
+        return ok;
     }
-    if (!ok) report_error(st, STAGE_LR, (unsigned long long)i, VACO_AV1_MSG_LR_COEFFICIENT);
+    if (u.type == VACO_AV1_LR_SGRPROJ)
+        return u.set >= 0 && u.set < 16 && u.xqd[0] >= -96 && u.xqd[0] <= 31 && u.xqd[1] >= -32 && u.xqd[1] <= 95;
+    return false;
+}
+
+// RestorationUnit::validate (restoration.rs:67-91).
+__global__ void lr_unit_check_kernel(const vaco_av1_lr_unit* units, int n, int plane, DeviceStatus* st) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!unit_ok(units[i]))
+        report_error(st, STAGE_LR, lr_key_position(plane, LRC_COEFFICIENT, i), VACO_AV1_MSG_LR_COEFFICIENT);
+}
+
+__global__ void lr_unit_check_batch_kernel(const UnitCheck* checks) {
+    const UnitCheck c = checks[blockIdx.y];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.count; i += gridDim.x * blockDim.x)
+        if (!unit_ok(c.units[i]))
+            report_error(c.status, STAGE_LR, lr_key_position(c.plane, LRC_COEFFICIENT, i), VACO_AV1_MSG_LR_COEFFICIENT);
 }
 
 __global__ void range_check_kernel(DevPlaneC p, int w, int h, int maxv, DeviceStatus* st, unsigned stage,
@@ -313,9 +362,12 @@ __global__ void range_check_kernel(DevPlaneC p, int w, int h, int maxv, DeviceSt
 
 }  // namespace
 
-cudaError_t launch_restoration(const LrPlane* planes, int count, int bit_depth, cudaStream_t stream) {
-    if (count <= 0) return cudaSuccess;
+size_t lr_args_size() { return sizeof(LrArgs); }
+
+// Kernel arguments of up to 3 planes; returns the number of tiles.
+int build_lr_args(const LrPlane* planes, int count, int bit_depth, void* out) {
     LrArgs a;
+    memset(&a, 0, sizeof a);
     a.count = count;
     a.bit_depth = bit_depth;
     int total = 0;
@@ -331,25 +383,58 @@ cudaError_t launch_restoration(const LrPlane* planes, int count, int bit_depth, 
         a.tile_base[k] = total;
         total += a.tiles_x[k] * a.tiles_y[k];
     }
-    a.tile_base[count] = total;
-    for (int k = count + 1; k < 4; ++k) a.tile_base[k] = total;
-    // The opt-in above 48 KB of dynamic shared memory is a per-device attribute.
+    for (int k = count; k < 4; ++k) a.tile_base[k] = total;
+    memcpy(out, &a, sizeof a);
+    return total;
+}
+
+// The opt-in above 48 KB of dynamic shared memory is a per-device attribute.
+cudaError_t lr_kernel_attributes() {
     static unsigned long long attr_devices = 0;
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && !(attr_devices & (1ull << dev))) {
         cudaError_t e = cudaFuncSetAttribute(restoration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)kLrSmem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(restoration_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kLrSmem);
         if (e != cudaSuccess) return e;
         attr_devices |= 1ull << dev;
     }
-    restoration_kernel<<<total, kLrThreads, kLrSmem, stream>>>(a);
+    return cudaSuccess;
+}
+
+cudaError_t launch_restoration(const LrPlane* planes, int count, int bit_depth, cudaStream_t stream) {
+    if (count <= 0) return cudaSuccess;
+    LrArgs a;
+    const int total = build_lr_args(planes, count, bit_depth, &a);
+    cudaError_t e = lr_kernel_attributes();
+    if (e != cudaSuccess) return e;
+    if (total > 0) restoration_kernel<<<total, kLrThreads, kLrSmem, stream>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_lr_unit_check(const vaco_av1_lr_unit* units, int n, DeviceStatus* status, cudaStream_t stream) {
+cudaError_t launch_restoration_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, int grid,
+                                     cudaStream_t stream) {
+    cudaError_t e = lr_kernel_attributes();
+    if (e != cudaSuccess) return e;
+    restoration_batch_kernel<<<grid, kLrThreads, kLrSmem, stream>>>(static_cast<const LrArgs*>(dev_args), dev_prefix,
+                                                                    n, dev_queue);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lr_unit_check(const vaco_av1_lr_unit* units, int n, int plane, DeviceStatus* status,
+                                 cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
-    lr_unit_check_kernel<<<div_up(n, 128), 128, 0, stream>>>(units, n, status);
+    lr_unit_check_kernel<<<div_up(n, 128), 128, 0, stream>>>(units, n, plane, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lr_unit_check_batch(const UnitCheck* dev_checks, int n, int max_count, cudaStream_t stream) {
+    if (n <= 0 || max_count <= 0) return cudaSuccess;
+    dim3 grid(std::min(div_up(max_count, 128), 64), n);
+    lr_unit_check_batch_kernel<<<grid, 128, 0, stream>>>(dev_checks);
     return cudaGetLastError();
 }
 

@@ -157,6 +157,41 @@ class Context:
         st = lib().vaco_av1_postfilter_frame_dev(self.handle, stream, C.byref(dev.job), C.byref(m))
         _check(self, st, m)
 
+    # ------------------------------------------------------------ batched form
+    @property
+    def tuning(self) -> abi.Tuning:
+        t = abi.Tuning()
+        lib().vaco_av1_ctx_get_tuning(self.handle, C.byref(t))
+        return t
+
+    def set_tuning(self, dbcdef_ctas_per_sm=None, lr_ctas_per_sm=None, use_graphs=None, largest_first=None):
+        t = self.tuning
+        for name, v in (("dbcdef_ctas_per_sm", dbcdef_ctas_per_sm), ("lr_ctas_per_sm", lr_ctas_per_sm),
+                        ("use_graphs", use_graphs), ("largest_first", largest_first)):
+            if v is not None:
+                setattr(t, name, int(v))
+        st = lib().vaco_av1_ctx_set_tuning(self.handle, C.byref(t))
+        if st != abi.OK:
+            raise VacoError(st, 0, "invalid tuning")
+
+    def batch_jobs(self, frames: Sequence["DeviceFrame"]):
+        arr = (abi.FrameJob * len(frames))()
+        for i, d in enumerate(frames):
+            arr[i] = d.job
+        return arr
+
+    def postfilter_batch_dev(self, frames: Sequence["DeviceFrame"], stream=None, jobs=None):
+        """The chain over many device-resident frames in one launch set;
+        returns per-frame (status, msg) lists."""
+        n = len(frames)
+        jobs = jobs if jobs is not None else self.batch_jobs(frames)
+        st = (C.c_int32 * n)()
+        ms = (C.c_int32 * n)()
+        rc = lib().vaco_av1_postfilter_batch_dev(self.handle, stream, jobs, n, st, ms)
+        if rc == abi.DEVICE_ERROR:
+            raise VacoError(rc, abi.MSG["CUDA"], f"cudaError={lib().vaco_av1_ctx_last_cuda_error(self.handle)}")
+        return list(st), list(ms)
+
 
 class DeviceFrame:
     """A FrameInputs uploaded to device memory (torch tensors) with its output
