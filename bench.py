@@ -429,6 +429,7 @@ def main():
     ap.add_argument("--workload", default="chain_4k_10bit", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--mode", default="headline", choices=["headline", "batch", "serve"])
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="seconds per arrival rate in --mode serve")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_env()

@@ -366,6 +366,89 @@ VACO_AV1_API int32_t vaco_av1_ctx_get_tuning(const vaco_av1_ctx* ctx, vaco_av1_t
 VACO_AV1_API int32_t vaco_av1_postfilter_batch_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_frame_job* jobs,
                                                    int32_t n, int32_t* statuses, int32_t* msgs);
 
+/* ---------------------------------------------------------------- served form */
+
+/* A request server (no counterpart in vaco): many decoder streams submit
+ * frames as they are reconstructed; a worker thread packs every pending frame
+ * into the next batched launch set as soon as one of its in-flight slots is
+ * free (continuous batching), so frames that arrive while others are on the
+ * GPU are admitted as slots free up and their work overlaps on the device.
+ * Each stream's frame buffers live in device memory for the stream's
+ * lifetime, admitted against a device-memory budget. */
+typedef struct vaco_av1_server vaco_av1_server;
+
+typedef struct vaco_av1_server_config {
+    int32_t device;
+    int32_t max_batch_frames;     /* frames packed into one launch set */
+    int32_t inflight_batches;     /* launch sets in flight (one CUDA stream each) */
+    int32_t reserved;
+    int64_t memory_budget_bytes;  /* stream buffers + batch scratch */
+} vaco_av1_server_config;
+
+typedef struct vaco_av1_server_stats {
+    uint64_t submitted;
+    uint64_t completed;
+    uint64_t failed;
+    uint64_t batches;
+    uint64_t max_batch;           /* largest launch set so far */
+    int64_t resident_bytes;       /* stream buffers currently admitted */
+    int64_t scratch_bytes;        /* batch scratch reserved per in-flight slot x slots */
+} vaco_av1_server_stats;
+
+VACO_AV1_API int32_t vaco_av1_server_create(const vaco_av1_server_config* config, vaco_av1_server** out);
+VACO_AV1_API void vaco_av1_server_destroy(vaco_av1_server* server);
+
+/* Admits a stream of frames with geometry `info` (4:2:0 or any layout the
+ * chain accepts) and restoration unit sizes lr_unit_size[3] (0 = no
+ * restoration for that plane), holding `buffers` frame slots resident on the
+ * device.  Fails with VACO_AV1_LIMIT_EXCEEDED / VACO_AV1_MSG_QUEUE_FULL when
+ * the budget cannot hold the stream's buffers. */
+VACO_AV1_API int32_t vaco_av1_server_open_stream(vaco_av1_server* server, const vaco_av1_frame_info* info,
+                                                 const int32_t* lr_unit_size, int32_t buffers, int32_t* stream_id,
+                                                 int32_t* msg);
+VACO_AV1_API int32_t vaco_av1_server_close_stream(vaco_av1_server* server, int32_t stream_id);
+
+/* Device pointers of slot `slot` of a stream, filled into `job` (src and dst
+ * pictures, side-information arrays, unit arrays): the decoder writes the
+ * reconstruction and side information there before submitting the slot. */
+VACO_AV1_API int32_t vaco_av1_server_slot(vaco_av1_server* server, int32_t stream_id, int32_t slot,
+                                          vaco_av1_frame_job* job);
+
+/* Queues slot `slot` of a stream with the frame-level parameters of `params`
+ * (deblock, cdef, lr_type; its pointers and geometry are ignored) and returns
+ * a ticket.  Does not wait for the GPU, except that a slot whose previous
+ * frame is still being filtered is waited for first (backpressure, at most
+ * 10 s, then VACO_AV1_TIMEOUT). */
+VACO_AV1_API int32_t vaco_av1_server_submit(vaco_av1_server* server, int32_t stream_id, int32_t slot,
+                                            const vaco_av1_frame_job* params, uint64_t* ticket);
+
+/* Waits up to timeout_ms (< 0: forever) for a ticket.  Returns VACO_AV1_TIMEOUT
+ * if it has not completed; otherwise the frame's status, with the message and
+ * the submit-to-completion latency in milliseconds.  A completed ticket is
+ * released by this call. */
+VACO_AV1_API int32_t vaco_av1_server_wait(vaco_av1_server* server, uint64_t ticket, int32_t timeout_ms,
+                                          int32_t* msg, double* latency_ms);
+
+VACO_AV1_API int32_t vaco_av1_server_get_stats(vaco_av1_server* server, vaco_av1_server_stats* stats);
+
+/* Bulk forms of submit / wait for clients that feed many streams from one
+ * thread: entry i is (stream_ids[i], slots[i], params[i]) -> tickets[i]. */
+VACO_AV1_API int32_t vaco_av1_server_submit_many(vaco_av1_server* server, int32_t n, const int32_t* stream_ids,
+                                                 const int32_t* slots, const vaco_av1_frame_job* params,
+                                                 uint64_t* tickets);
+VACO_AV1_API int32_t vaco_av1_server_wait_many(vaco_av1_server* server, int32_t n, const uint64_t* tickets,
+                                               int32_t timeout_ms, int32_t* statuses, int32_t* msgs,
+                                               double* latency_ms);
+
+/* Host-memory conveniences around vaco_av1_server_slot(): copy a frame's
+ * reconstruction, side information and restoration units from host arrays
+ * (`host` uses host pointers; extents must match the stream) into a slot, and
+ * copy a completed slot's output planes back.  Both are synchronous. */
+VACO_AV1_API int32_t vaco_av1_server_upload(vaco_av1_server* server, int32_t stream_id, int32_t slot,
+                                            const vaco_av1_frame_job* host);
+VACO_AV1_API int32_t vaco_av1_server_download(vaco_av1_server* server, int32_t stream_id, int32_t slot,
+                                              const vaco_av1_picture* host);
+
 /* The whole chain for callers that cannot call cudaMalloc.  No counterpart in
  * vaco (vaco allocates every intermediate picture through its Budget).
  *

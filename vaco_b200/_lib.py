@@ -42,6 +42,18 @@ SIGNATURES = [
     ("vaco_av1_ctx_get_tuning", _i32, [_vp, _vp]),
     ("vaco_av1_postfilter_batch_dev", _i32, [_vp, _vp, _vp, _i32, _vp, _vp]),
     ("vaco_av1_postfilter_frame_noalloc", _i32, [_vp, _vp, _pi32]),
+    ("vaco_av1_server_create", _i32, [_vp, _vp]),
+    ("vaco_av1_server_destroy", None, [_vp]),
+    ("vaco_av1_server_open_stream", _i32, [_vp, _vp, _vp, _i32, _vp, _vp]),
+    ("vaco_av1_server_close_stream", _i32, [_vp, _i32]),
+    ("vaco_av1_server_slot", _i32, [_vp, _i32, _i32, _vp]),
+    ("vaco_av1_server_submit", _i32, [_vp, _i32, _i32, _vp, _vp]),
+    ("vaco_av1_server_wait", _i32, [_vp, C.c_uint64, _i32, _vp, _vp]),
+    ("vaco_av1_server_get_stats", _i32, [_vp, _vp]),
+    ("vaco_av1_server_upload", _i32, [_vp, _i32, _i32, _vp]),
+    ("vaco_av1_server_download", _i32, [_vp, _i32, _i32, _vp]),
+    ("vaco_av1_server_submit_many", _i32, [_vp, _i32, _vp, _vp, _vp, _vp]),
+    ("vaco_av1_server_wait_many", _i32, [_vp, _i32, _vp, _i32, _vp, _vp, _vp]),
 ]
 
 _lib = None

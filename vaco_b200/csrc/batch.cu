@@ -118,12 +118,13 @@ extern "C" int32_t vaco_av1_ctx_get_tuning(const vaco_av1_ctx* ctx, vaco_av1_tun
     return VACO_AV1_OK;
 }
 
-extern "C" int32_t vaco_av1_postfilter_batch_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_frame_job* jobs,
-                                                 int32_t n, int32_t* statuses, int32_t* msgs) {
-    if (!ctx || (n > 0 && !jobs)) return VACO_AV1_INVALID_DATA;
-    if (n <= 0) return VACO_AV1_OK;
+// Enqueues the whole batch on `s` without waiting; `pending` keeps what
+// batch_collect() needs once the stream has passed the batch.
+int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_frame_job* jobs, int n,
+                            BatchPending* pending) {
+    int32_t* statuses = nullptr;
+    int32_t* msgs = nullptr;
     cudaSetDevice(ctx->device);
-    cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaSuccess;
     if (!ctx->sm_count) {
         e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
@@ -435,20 +436,47 @@ extern "C" int32_t vaco_av1_postfilter_batch_dev(vaco_av1_ctx* ctx, void* stream
     }
     ctx->launches += launches;
     if (e == cudaSuccess) ctx->mark(1, s), ctx->mark(2, s), ctx->mark(3, s), ctx->mark(4, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(ctx, e, statuses, msgs, n);
-    ctx->collect_marks();
-
-    // ---- per-frame results
-    int32_t first = VACO_AV1_OK;
+    pending->n = n;
+    pending->host_keys.resize(n);
+    pending->queued.resize(n);
     for (int i = 0; i < n; ++i) {
-        unsigned long long key = ctx->batch_status_host[i];
-        if (!plan[i].run_db) key = kNoError;  // never queued: its word is untouched
-        if (plan[i].host_key < key) key = plan[i].host_key;
+        pending->host_keys[i] = plan[i].host_key;
+        pending->queued[i] = plan[i].run_db ? 1 : 0;
+    }
+    return VACO_AV1_OK;
+}
+
+// Per-frame results of a batch whose stream work has completed.
+int32_t vaco::batch_collect(vaco_av1_ctx* ctx, const BatchPending& pending, int32_t* statuses, int32_t* msgs) {
+    ctx->collect_marks();
+    int32_t first = VACO_AV1_OK;
+    for (int i = 0; i < pending.n; ++i) {
+        unsigned long long key = pending.queued[i] ? ctx->batch_status_host[i] : kNoError;
+        if (pending.host_keys[i] < key) key = pending.host_keys[i];
         const int32_t st = key == kNoError ? VACO_AV1_OK : VACO_AV1_INVALID_DATA;
         if (statuses) statuses[i] = st;
         if (msgs) msgs[i] = key == kNoError ? 0 : (int32_t)(key & 0xFF);
         if (first == VACO_AV1_OK && st != VACO_AV1_OK) first = st;
     }
     return first;
+}
+
+extern "C" int32_t vaco_av1_postfilter_batch_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_frame_job* jobs,
+                                                 int32_t n, int32_t* statuses, int32_t* msgs) {
+    if (!ctx || (n > 0 && !jobs)) return VACO_AV1_INVALID_DATA;
+    if (n <= 0) return VACO_AV1_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    BatchPending pending;
+    int32_t st = batch_enqueue(ctx, s, jobs, n, &pending);
+    if (st != VACO_AV1_OK) {
+        for (int i = 0; i < n; ++i) {
+            if (statuses) statuses[i] = st;
+            if (msgs) msgs[i] = VACO_AV1_MSG_CUDA;
+        }
+        return st;
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(ctx, e, statuses, msgs, n);
+    return batch_collect(ctx, pending, statuses, msgs);
 }

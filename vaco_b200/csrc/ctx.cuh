@@ -6,6 +6,8 @@
 
 #include "common.cuh"
 
+#include <vector>
+
 namespace vaco {
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 }  // namespace vaco
@@ -83,3 +85,14 @@ enum Slot {
     S_BATCH_ARENA, S_BATCH_TABLE,      // batched form: intermediates, per-batch tables
 };
 
+
+namespace vaco {
+// Asynchronous halves of vaco_av1_postfilter_batch_dev (batch.cu).
+struct BatchPending {
+    int n = 0;
+    std::vector<unsigned long long> host_keys;
+    std::vector<int> queued;  // frames whose device status word is live
+};
+int32_t batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_frame_job* jobs, int n, BatchPending* pending);
+int32_t batch_collect(vaco_av1_ctx* ctx, const BatchPending& pending, int32_t* statuses, int32_t* msgs);
+}  // namespace vaco
