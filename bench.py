@@ -81,7 +81,13 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark_start(self):
+        self.t_start = time.time()
+
+    def mark_end(self):
+        self.t_end = time.time()
 
     def stop(self):
         if not self.proc:
@@ -94,7 +100,11 @@ class ClockSampler:
         self.thread.join(timeout=2)
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0, t1 = getattr(self, "t_start", 0.0), getattr(self, "t_end", float("inf"))
+        timed = [ln for ts, ln in self.lines if t0 <= ts <= t1]
+        if not timed and self.lines:  # region shorter than one sampling period
+            timed = [min(self.lines, key=lambda x: abs(x[0] - (t0 + t1) / 2))[1]]
+        for ln in timed:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
                 continue
@@ -258,19 +268,21 @@ def run_gpu(args, world, rank, local):
         return float(t.item())
 
     # -------- device-resident throughput
+    clocks = ClockSampler(local)
+    clocks.start()  # sampling runs from before warm-up; only timed-region samples count
     for i in range(args.warmup):
         step(i)
     lib().vaco_av1_ctx_set_stage_timing(ctx.handle, 1)
     launches0 = ctx.launches
-    clocks = ClockSampler(local)
     barrier()
-    clocks.start()
+    clocks.mark_start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for i in range(args.steps):
         step(i)
     ev1.record(stream)
     barrier()
+    clocks.mark_end()
     clock_info = clocks.stop()
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     launches = ctx.launches - launches0
@@ -423,7 +435,7 @@ def run_batch(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=8000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="vaco_b200", choices=["vaco_b200", "reference"])
     ap.add_argument("--workload", default="chain_4k_10bit", choices=sorted(WORKLOADS))

@@ -591,6 +591,8 @@ int32_t vaco_av1_restore_plane_dev(vaco_av1_ctx* ctx, void* stream, const uint16
     p.unit_cols = cols;
     p.unit_rows = rows;
     p.copy_only = 0;
+    p.plane_index = 0;
+    p.unit_status = nullptr;  // validated by the checks above
     e = launch_restoration(&p, 1, config->bit_depth, s);
     ctx->launches++;
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
@@ -733,12 +735,7 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
             rows_like.height[k] = pre_rows_count(job->src.height[k], k ? ssy : 0);
         }
         if (!alloc_picture(ctx, &rows_like, np, S_PRE0, &pre_rows, &e)) return cuda_fail(ctx, e, msg);
-        for (int k = 0; k < np; ++k) {
-            pre_rows_dp[k] = mplane(pre_rows, k);
-            // rows past the frame bottom are never written; keep them defined
-            e = cudaMemsetAsync(pre_rows.planes[k], 0, (size_t)pre_rows.stride[k] * pre_rows.height[k] * 2, s);
-            if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
-        }
+        for (int k = 0; k < np; ++k) pre_rows_dp[k] = mplane(pre_rows, k);
     }
     ctx->mark(0, s);
 
@@ -810,10 +807,13 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
         after = ucdef;
         if (lr_active) {
             if (!alloc_picture(ctx, &rows_out_like, np, S_UPRE0, &urows, &e)) return cuda_fail(ctx, e, msg);
+            // only the rows the fused kernel wrote (indices 4 .. 4+n)
             for (int k = 0; k < np; ++k) {
-                sp[k].in = cplane(pre_rows, k);
-                sp[k].out = mplane(urows, k);
-                sp[k].height = pre_rows.height[k];
+                const int n_rows = pre_rows_written(job->src.height[k], k ? ssy : 0);
+                sp[k].in = DevPlaneC{pre_rows.planes[k] + 4L * pre_rows.stride[k], pre_rows.width[k], n_rows,
+                                     pre_rows.stride[k]};
+                sp[k].out = DevPlane{urows.planes[k] + 4L * urows.stride[k], urows.width[k], n_rows, urows.stride[k]};
+                sp[k].height = n_rows;
             }
             e = launch_superres(sp, np, info.bit_depth, ctx->status, STAGE_SUPERRES, s);
             ctx->launches++;
@@ -850,10 +850,9 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
                 hk = make_key(STAGE_LR, lr_position(k, LR_COUNT, 0), VACO_AV1_MSG_NULL_ARGUMENT);
                 break;
             }
-            e = launch_lr_unit_check(job->lr_units[k], job->lr_unit_count[k], k, ctx->status, s);
-            ctx->launches++;
-            if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
             LrPlane& p = lp[nlr++];
+            p.plane_index = k;
+            p.unit_status = ctx->status;  // units are validated by the restoration tiles
             p.before = DevPlaneC{nullptr, 0, 0, 0};
             p.before_rows = cplane(before_rows, k);
             p.after = cplane(after, k);

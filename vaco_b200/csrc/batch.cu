@@ -4,16 +4,15 @@
 // src/decode.rs:553-559).  Here a batch of frames of any sizes and bit depths
 // shares one launch set:
 //   1. one upload of the per-batch tables (frame argument records, tile
-//      prefix sums, unit-check list, initial status words, queue counters)
-//   2. one unit-check kernel for every restoration unit array of the batch
-//   3. one persistent deblock+CDEF kernel draining a device tile queue that
+//      prefix sums, initial status words, queue counters)
+//   2. one persistent deblock+CDEF kernel draining a device tile queue that
 //      spans all frames (dbcdef.cu)
-//   4. superres launches for the frames that upscale
-//   5. one persistent restoration kernel over all frames' tiles
-//      (restoration.cu), which also copies planes whose frame-level
-//      restoration is off
-//   6. one download of the per-frame status words
-// With tuning.use_graphs, steps 1-6 are captured once per batch composition as
+//   3. superres launches for the frames that upscale
+//   4. one persistent restoration kernel over all frames' tiles
+//      (restoration.cu), which also validates every restoration unit and
+//      copies planes whose frame-level restoration is off
+//   5. one download of the per-frame status words
+// With tuning.use_graphs, steps 1-5 are captured once per batch composition as
 // a CUDA graph and replayed afterwards; the tables carry every per-batch
 // pointer, so a replay only needs the host to refresh the pinned staging copy.
 #include <algorithm>
@@ -134,7 +133,6 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     // ---- host pass: checks, scratch layout, tile counts
     std::vector<FramePlan> plan(n);
     Arena arena;
-    size_t rows_begin = 0, rows_end = 0;
     std::string signature = std::to_string(n) + ":";
     for (int i = 0; i < n; ++i) {
         const vaco_av1_frame_job& J = jobs[i];
@@ -199,15 +197,13 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
         for (int k = 0; k < F.np; ++k) signature += std::to_string(J.lr_type[k]) + "," + std::to_string(J.lr_unit_size[k]);
         signature += ";";
     }
-    // boundary rows of every frame in one contiguous range (one memset)
-    rows_begin = arena.used;
+    // boundary rows (restoration's pre-CDEF source) of every frame
     for (int i = 0; i < n; ++i) {
         FramePlan& F = plan[i];
         if (!F.run_db || !F.lr_active) continue;
         for (int k = 0; k < F.np; ++k)
             F.rows[k] = arena.take(jobs[i].src.width[k], pre_rows_count(jobs[i].src.height[k], k ? jobs[i].info.subsampling_y : 0));
     }
-    rows_end = arena.used;
     for (int i = 0; i < n; ++i) {
         FramePlan& F = plan[i];
         if (!F.run_db || !F.superres) continue;
@@ -247,8 +243,6 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     off = align_up(off + lr_rec * lr_order.size(), 256);
     const size_t off_lr_prefix = off;
     off = align_up(off + sizeof(int) * (lr_order.size() + 1), 256);
-    const size_t off_checks = off;
-    off = align_up(off + sizeof(UnitCheck) * 3 * lr_order.size(), 256);
     const size_t table_bytes = off;
     unsigned char* dtab = static_cast<unsigned char*>(ctx->scratch(S_BATCH_TABLE, table_bytes));
     if (!dtab) return fail(ctx, cudaErrorMemoryAllocation, statuses, msgs, n);
@@ -317,8 +311,6 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     // restoration records and unit checks
     int* lr_prefix = reinterpret_cast<int*>(htab + off_lr_prefix);
     lr_prefix[0] = 0;
-    UnitCheck* checks = reinterpret_cast<UnitCheck*>(htab + off_checks);
-    int n_checks = 0, max_units = 0;
     for (size_t q = 0; q < lr_order.size(); ++q) {
         const int i = lr_order[q];
         const FramePlan& F = plan[i];
@@ -330,6 +322,8 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
             const int w = info.upscaled_width >> sx, h = info.coded_height >> sy;
             const PlaneBuf& after = F.superres ? F.ucdef[k] : F.cdef[k];
             LrPlane& p = lp[k];
+            p.plane_index = k;
+            p.unit_status = dstatus + i;  // units are validated by the restoration tiles
             p.before = DevPlaneC{nullptr, 0, 0, 0};
             p.after = dev_cplane(base, after);
             p.out = DevPlane{J.dst.planes[k], w, h, J.dst.stride[k]};
@@ -350,8 +344,7 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
                 p.unit_cols = std::max((w + u / 2) / u, 1);
                 p.unit_rows = std::max((h + u / 2) / u, 1);
                 p.copy_only = 0;
-                checks[n_checks++] = UnitCheck{J.lr_units[k], J.lr_unit_count[k], k, dstatus + i};
-                max_units = std::max(max_units, J.lr_unit_count[k]);
+
             }
         }
         const int tiles = build_lr_args(lp, F.np, info.bit_depth, htab + off_lr + lr_rec * q);
@@ -363,10 +356,6 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     const int grid_lr = std::max(1, ctx->sm_count * ctx->tuning.lr_ctas_per_sm);
     auto enqueue = [&]() -> cudaError_t {
         cudaError_t r = cudaMemcpyAsync(dtab, htab, table_bytes, cudaMemcpyHostToDevice, s);
-        if (r == cudaSuccess && rows_end > rows_begin)
-            r = cudaMemsetAsync(base + rows_begin, 0, rows_end - rows_begin, s);
-        if (r == cudaSuccess && n_checks)
-            r = launch_lr_unit_check_batch(reinterpret_cast<const UnitCheck*>(dtab + off_checks), n_checks, max_units, s);
         if (r == cudaSuccess && !order.empty() && db_prefix[order.size()] > 0)
             r = launch_dbcdef_batch(dtab + off_db, reinterpret_cast<const int*>(dtab + off_db_prefix), (int)order.size(),
                                     reinterpret_cast<int*>(dtab + off_queue), smem_db, grid_db, s);
@@ -385,10 +374,17 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
             }
             r = launch_superres(sp, F.np, info.bit_depth, dstatus + i, STAGE_SUPERRES, s);
             if (r == cudaSuccess && F.lr_active && F.run_lr) {
+                // only the rows the fused kernel wrote (indices 4 .. 4+n)
                 for (int k = 0; k < F.np; ++k) {
-                    sp[k].in = dev_cplane(base, F.rows[k]);
-                    sp[k].out = dev_plane(base, F.urows[k]);
-                    sp[k].height = F.rows[k].h;
+                    const int n_rows = pre_rows_written(jobs[i].src.height[k], k ? info.subsampling_y : 0);
+                    DevPlaneC in = dev_cplane(base, F.rows[k]);
+                    DevPlane out = dev_plane(base, F.urows[k]);
+                    in.data += 4L * in.stride;
+                    out.data += 4L * out.stride;
+                    in.height = out.height = n_rows;
+                    sp[k].in = in;
+                    sp[k].out = out;
+                    sp[k].height = n_rows;
                 }
                 r = launch_superres(sp, F.np, info.bit_depth, dstatus + i, STAGE_SUPERRES, s);
             }
@@ -401,8 +397,8 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
                                 s);
         return r;
     };
-    // kernel launches of this batch: unit check, deblock+CDEF, superres, restoration
-    size_t launches = (n_checks ? 1 : 0) + (order.empty() ? 0 : 1) + (lr_order.empty() ? 0 : 1);
+    // kernel launches of this batch: deblock+CDEF, superres, restoration
+    size_t launches = (order.empty() ? 0 : 1) + (lr_order.empty() ? 0 : 1);
     for (int i : order) launches += plan[i].superres ? (plan[i].lr_active && plan[i].run_lr ? 2 : 1) : 0;
     ctx->mark(0, s);
     const bool graphs = ctx->tuning.use_graphs && s != nullptr;

@@ -48,6 +48,8 @@ struct LrPlane {
     const vaco_av1_lr_unit* units;  // device
     int unit_cols, unit_rows;
     int copy_only;                  // 1: output = `after` (frame-level restoration off for the plane)
+    int plane_index;                // 0 = Y, 1 = U, 2 = V (status-word key of unit checks)
+    DeviceStatus* unit_status;      // non-null: validate each tile's unit here (restoration.rs:67-91)
 };
 // Restores up to 3 planes in one launch.  Units must have been validated.
 cudaError_t launch_restoration(const LrPlane* planes, int count, int bit_depth, cudaStream_t stream);
@@ -57,7 +59,6 @@ size_t lr_args_size();
 int build_lr_args(const LrPlane* planes, int count, int bit_depth, void* out);
 cudaError_t launch_restoration_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, int grid,
                                      cudaStream_t stream);
-// Reports VACO_AV1_MSG_LR_COEFFICIENT for invalid units of many unit arrays.
 // Shared-memory opt-ins of every kernel on the current device (idempotent);
 // call before stream capture.
 cudaError_t dbcdef_kernel_attributes();
@@ -66,13 +67,7 @@ inline cudaError_t kernel_attributes() {
     cudaError_t e = dbcdef_kernel_attributes();
     return e == cudaSuccess ? lr_kernel_attributes() : e;
 }
-struct UnitCheck {
-    const vaco_av1_lr_unit* units;
-    int count;
-    int plane;
-    DeviceStatus* status;
-};
-cudaError_t launch_lr_unit_check_batch(const UnitCheck* dev_checks, int n, int max_count, cudaStream_t stream);
+
 // Reports VACO_AV1_MSG_LR_COEFFICIENT for the first invalid unit of `plane`,
 // keyed after that plane's geometry/count checks and before its sample checks.
 cudaError_t launch_lr_unit_check(const vaco_av1_lr_unit* units, int n, int plane, DeviceStatus* status,
@@ -134,6 +129,16 @@ cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int
 inline int pre_rows_count(int height, int sub_y) {
     const int sh = 64 >> sub_y, off = 8 >> sub_y;
     return 4 * ((height + off + 2) / sh + 1);
+}
+// Rows of that buffer the fused kernel writes: indices [4, 4 + n) hold the
+// plane rows k*stripe - offset - 2 + sub (k >= 1, sub < 4) that lie inside
+// the plane; restoration reads no other index.
+inline int pre_rows_written(int height, int sub_y) {
+    const int sh = 64 >> sub_y, off = 8 >> sub_y;
+    int n = 0;
+    for (int i = 4; i < pre_rows_count(height, sub_y); ++i)
+        if ((i >> 2) * sh - off - 2 + (i & 3) < height) ++n;
+    return n;
 }
 
 }  // namespace vaco

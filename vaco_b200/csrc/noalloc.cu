@@ -291,6 +291,8 @@ extern "C" int32_t vaco_av1_postfilter_frame_noalloc(void* stream, const vaco_av
             LrPlane& p = lp[nlr++];
             p.before = DevPlaneC{before[k].data, before[k].width, before[k].height, before[k].stride};
             p.before_rows = DevPlaneC{nullptr, 0, 0, 0};
+            p.plane_index = k;
+            p.unit_status = nullptr;  // validated by the unit check above
             p.after = DevPlaneC{after[k].data, after[k].width, after[k].height, after[k].stride};
             p.out = DevPlane{J.dst.planes[k], w, h, J.dst.stride[k]};
             p.width = w;

@@ -71,6 +71,22 @@ constexpr size_t kLrSmem = kSBytes + kRegion + 256 * sizeof(uint16_t);
 
 __device__ __forceinline__ int round2i(int v, int s) { return s == 0 ? v : (v + (1 << (s - 1))) >> s; }
 
+__device__ __forceinline__ bool unit_ok(const vaco_av1_lr_unit& u) {
+    if (u.type == VACO_AV1_LR_NONE) return true;
+    if (u.type == VACO_AV1_LR_WIENER) {
+        const int lo[3] = {-5, -23, -17}, hi[3] = {10, 8, 46};
+        bool ok = true;
+        for (int k = 0; k < 3; ++k)
+            ok = ok && u.vertical[k] >= lo[k] && u.vertical[k] <= hi[k] && u.horizontal[k] >= lo[k] &&
+                 u.horizontal[k] <= hi[k];
+        return ok;
+    }
+    if (u.type == VACO_AV1_LR_SGRPROJ)
+        return u.set >= 0 && u.set < 16 && u.xqd[0] >= -96 && u.xqd[0] <= 31 && u.xqd[1] >= -32 && u.xqd[1] <= 95;
+    return false;
+}
+
+
 // Box sums around every position of one row band and the a2 / b terms of
 // box_ab (restoration.rs:314-339).
 template <int RAD>
@@ -138,8 +154,17 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     const int urow = min((y_lo + off) / P.unit_size, P.unit_rows - 1);
     const int ucol = min(x_lo / P.unit_size, P.unit_cols - 1);
     vaco_av1_lr_unit u;
-    if (P.copy_only) u.type = VACO_AV1_LR_NONE;
-    else u = P.units[urow * P.unit_cols + ucol];
+    if (P.copy_only) {
+        u.type = VACO_AV1_LR_NONE;
+    } else {
+        const int ui = urow * P.unit_cols + ucol;
+        u = P.units[ui];
+        // Every unit is covered by at least one tile, so checking each tile's
+        // unit validates the whole unit array (RestorationUnit::validate).
+        if (P.unit_status && tid == 0 && !unit_ok(u))
+            report_error(P.unit_status, STAGE_LR, lr_key_position(P.plane_index, LRC_COEFFICIENT, ui),
+                         VACO_AV1_MSG_LR_COEFFICIENT);
+    }
     const int bd = a.bit_depth, maxv = (1 << bd) - 1;
 
     if (P.copy_only || (u.type != VACO_AV1_LR_WIENER && u.type != VACO_AV1_LR_SGRPROJ)) {
@@ -319,34 +344,12 @@ __global__ void __launch_bounds__(kLrThreads, 4) restoration_batch_kernel(const 
     }
 }
 
-__device__ __forceinline__ bool unit_ok(const vaco_av1_lr_unit& u) {
-    if (u.type == VACO_AV1_LR_NONE) return true;
-    if (u.type == VACO_AV1_LR_WIENER) {
-        const int lo[3] = {-5, -23, -17}, hi[3] = {10, 8, 46};
-        bool ok = true;
-        for (int k = 0; k < 3; ++k)
-            ok = ok && u.vertical[k] >= lo[k] && u.vertical[k] <= hi[k] && u.horizontal[k] >= lo[k] &&
-                 u.horizontal[k] <= hi[k];
-        return ok;
-    }
-    if (u.type == VACO_AV1_LR_SGRPROJ)
-        return u.set >= 0 && u.set < 16 && u.xqd[0] >= -96 && u.xqd[0] <= 31 && u.xqd[1] >= -32 && u.xqd[1] <= 95;
-    return false;
-}
-
 // RestorationUnit::validate (restoration.rs:67-91).
 __global__ void lr_unit_check_kernel(const vaco_av1_lr_unit* units, int n, int plane, DeviceStatus* st) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (!unit_ok(units[i]))
         report_error(st, STAGE_LR, lr_key_position(plane, LRC_COEFFICIENT, i), VACO_AV1_MSG_LR_COEFFICIENT);
-}
-
-__global__ void lr_unit_check_batch_kernel(const UnitCheck* checks) {
-    const UnitCheck c = checks[blockIdx.y];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.count; i += gridDim.x * blockDim.x)
-        if (!unit_ok(c.units[i]))
-            report_error(c.status, STAGE_LR, lr_key_position(c.plane, LRC_COEFFICIENT, i), VACO_AV1_MSG_LR_COEFFICIENT);
 }
 
 __global__ void range_check_kernel(DevPlaneC p, int w, int h, int maxv, DeviceStatus* st, unsigned stage,
@@ -428,13 +431,6 @@ cudaError_t launch_lr_unit_check(const vaco_av1_lr_unit* units, int n, int plane
                                  cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     lr_unit_check_kernel<<<div_up(n, 128), 128, 0, stream>>>(units, n, plane, status);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_lr_unit_check_batch(const UnitCheck* dev_checks, int n, int max_count, cudaStream_t stream) {
-    if (n <= 0 || max_count <= 0) return cudaSuccess;
-    dim3 grid(std::min(div_up(max_count, 128), 64), n);
-    lr_unit_check_batch_kernel<<<grid, 128, 0, stream>>>(dev_checks);
     return cudaGetLastError();
 }
 

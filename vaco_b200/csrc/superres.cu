@@ -103,6 +103,7 @@ cudaError_t launch_superres(const SuperresPlane* planes, int count, int bit_dept
     a.bit_depth = bit_depth;
     a.status = status;
     a.stage = stage;
+    if (max_w <= 0 || max_h <= 0) return cudaSuccess;  // nothing to upscale
     dim3 grid(div_up(max_w, kSrThreads), max_h, count);
     superres_kernel<<<grid, kSrThreads, 0, stream>>>(a);
     return cudaGetLastError();

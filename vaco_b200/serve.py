@@ -226,7 +226,7 @@ def plain_dropin_mixed(device=0, frames_per_res=4):
     for wl, _ in synth.BATCH_MIX:
         for i in range(frames_per_res):
             fs.append(synth.make_frame(wl, synth.seed_for(4, 7000 + len(fs))))
-    for f in fs[:4]:
+    for f in fs:  # warm: every frame size once (scratch and staging reach their final size)
         ctx.postfilter_frame(f)
     t0 = time.perf_counter()
     px = 0
