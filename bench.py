@@ -236,7 +236,7 @@ def run_gpu(args, world, rank, local):
 
     from vaco_b200 import abi
     from vaco_b200._lib import lib
-    from vaco_b200.frame import alloc_outputs, host_job
+    from vaco_b200.frame import pinned_copy
     from vaco_b200.gpu import Context, DeviceFrame
 
     torch.cuda.set_device(local)
@@ -295,19 +295,11 @@ def run_gpu(args, world, rank, local):
 
     # -------- end to end through the host entry point (pinned buffers)
     pinned_in, pinned_out, jobs = [], [], []
-    h2d = d2h = 0
     for f in frames[:2]:
-        pf = synth.FrameInputs(**{k: getattr(f, k) for k in f.__dataclass_fields__})
-        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
-        pf.planes = [pin(p) for p in f.planes]
-        pf.tx_luma, pf.tx_chroma, pf.skip = pin(f.tx_luma), pin(f.tx_chroma), pin(f.skip)
-        pf.cdef_idx = pin(f.cdef_idx)
-        pf.lvl_map = None if f.lvl_map is None else pin(f.lvl_map)
-        pf.lr_units = [pin(u.view(np.uint8)).view(u.dtype) for u in f.lr_units]
-        outs = [pin(o) for o in alloc_outputs(pf)]
+        pf, outs, job = pinned_copy(f)
         pinned_in.append(pf)
         pinned_out.append(outs)
-        jobs.append(host_job(pf, outs))
+        jobs.append(job)
     fin, fout, side = frame_bytes(frames[0])
     h2d = sum(p.nbytes for p in pinned_in[0].planes) + side
     d2h = sum(o.nbytes for o in pinned_out[0])

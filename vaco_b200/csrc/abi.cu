@@ -694,6 +694,7 @@ int32_t vaco_av1_deblock_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture*
 static bool chain_geometry_ok(const vaco_av1_frame_job* j) {
     const vaco_av1_frame_info& i = j->info;
     if (!info_ok(&i) || !padded_picture_ok(&j->src, &i)) return false;
+    if (!av1_subsampling_ok(i.subsampling_x, i.subsampling_y)) return false;
     if (i.coded_width <= 0 || i.coded_height <= 0 || i.coded_width > i.mi_cols * 4 || i.coded_height > i.mi_rows * 4)
         return false;
     if (i.mi_cols != 2 * ((i.coded_width + 7) >> 3) || i.mi_rows != 2 * ((i.coded_height + 7) >> 3)) return false;

@@ -38,7 +38,7 @@ bool depth_ok(int bd) { return bd == 8 || bd == 10 || bd == 12; }
 bool geometry_ok(const vaco_av1_frame_job& j) {
     const vaco_av1_frame_info& i = j.info;
     if (i.mi_rows <= 0 || i.mi_cols <= 0 || i.mi_rows > (1 << 15) || i.mi_cols > (1 << 15)) return false;
-    if (i.subsampling_x < 0 || i.subsampling_x > 1 || i.subsampling_y < 0 || i.subsampling_y > 1) return false;
+    if (!av1_subsampling_ok(i.subsampling_x, i.subsampling_y)) return false;
     if (i.coded_width <= 0 || i.coded_height <= 0) return false;
     if (i.mi_cols != 2 * ((i.coded_width + 7) >> 3) || i.mi_rows != 2 * ((i.coded_height + 7) >> 3)) return false;
     if (i.upscaled_width < i.coded_width) return false;

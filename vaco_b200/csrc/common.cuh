@@ -68,4 +68,11 @@ __host__ __device__ constexpr int tx_h_log2(int t) {
 
 inline int div_up(int a, int b) { return (a + b - 1) / b; }
 
+// Chroma layouts AV1 can signal (color_config, spec 5.5.2): 4:2:0, 4:2:2 and
+// 4:4:4.  subsampling_y is only coded when subsampling_x is 1, so 4:4:0 does
+// not exist; the fused deblock+CDEF tile layout relies on that.
+inline bool av1_subsampling_ok(int ssx, int ssy) {
+    return (ssx == 0 || ssx == 1) && (ssy == 0 || ssy == 1) && !(ssx == 0 && ssy == 1);
+}
+
 }  // namespace vaco

@@ -12,15 +12,17 @@
 //
 // Halo arithmetic (plane units, tile [x0, x0+tw) x [y0, y0+th)):
 //   CDEF reads the deblocked window [x0-2, x0+tw+2) x [y0-2, y0+th+2).
-//   Horizontal edges that modify window rows: E in [y0-4, y0+th+4] (a 14-tap
-//   filter modifies E-6..E+5); they read rows [E-7, E+6], i.e. [y0-11, y0+th+10].
-//   Vertical edges that modify window columns: X in [x0-4, x0+tw+4]; they read
-//   columns [x0-11, x0+tw+10].  The vertical pass runs on rows [y0-12,
-//   y0+th+12), which covers every row the horizontal pass reads.
-// The staged region is [x0-16, x0+tw+16) x [y0-16, y0+th+16).
-// Within a pass no two edges touch a common sample (see deblock.cu), so both
-// passes run one thread per edge line, in place; reads past the plane repeat
-// the edge sample and writes past it are dropped, as in deblock.cu.
+//   An edge of filter size n sits on a multiple of n (7.14.2: it is a
+//   transform edge of the block on its q side), and it modifies n/2 samples
+//   on either side at most (14-tap: 6, 8-tap: 3, 6-tap: 2, 4-tap: 2).  The
+//   edges that reach the window are therefore exactly the 4-aligned ones in
+//   [y0, y0+th] (horizontal) and [x0, x0+tw] (vertical); the edge at y0-4,
+//   say, is a size-4 edge and stops at y0-3.
+//   Those horizontal edges read rows [E-7, E+6] (luma, 14-tap only where E is
+//   a multiple of 16) or [E-3, E+2] (chroma, at most 6 taps): rows
+//   [y0-7, y0+th+7) for luma and [y0-3, y0+th+3) for chroma, which is where
+//   the vertical pass must run.  Vertical edges read columns [X-7, X+6].
+// The staged region is [x0-8, x0+tw+8) x [y0-8, y0+th+8).
 #include <algorithm>
 #include <cstring>
 
@@ -37,12 +39,12 @@ using namespace cdefk;
 using namespace dbk;
 
 constexpr int kThreads = 256;
-constexpr int kHalo = 16;
-// Segments per pass and plane are at most (th/4+4) x (tw/4+3) = 380.  Size
-// class lists: 0 = size 4 (any plane, up to 3 x 380), 1 = chroma size 8
-// (2 x 380), 2 = luma size 8 (380), 3 = luma size 16 (380).
-__constant__ int c_list_off[4] = {0, 1140, 1900, 2280};
-constexpr int kListTotal = 2660;
+constexpr int kHalo = 8;
+// Edge segments (one edge x one 4-sample cell) per pass and plane are at most
+// (th/4+4) x (tw/4+1) = 340.  Size-class lists: 0 = size 4 (any plane, up to
+// 3 x 340), 1 = chroma size 8 (2 x 340), 2 = luma size 8, 3 = luma size 16.
+__constant__ int c_list_off[4] = {0, 1020, 1700, 2040};
+constexpr int kListTotal = 2380;
 
 struct PlaneGeom {
     int tw, th;        // tile extent in this plane
@@ -131,6 +133,134 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const DevPlane& 
         for (int j = 0; j < BH / RPI; ++j)
             if (lr + RPI * j < rows_here) o[j * ostride] = cw[j * RPI * PITCH / 2];
     }
+}
+
+// Segment-list entry: level (6 bits) | samples on the q side, capped at 8 (4)
+// | on the p side, capped at 8 (4) | staged offset of q0 on the segment's
+// first line (13) | plane (2) | first cell of its edge (1) | last cell (1).
+// Capping at 8 keeps the clamping of load_line / store_at exact: no filter
+// reaches more than 7 samples from its edge.
+__device__ __forceinline__ uint32_t seg_entry(int lvl, int nq, int np, int off, int p, bool first, bool last) {
+    return (uint32_t)lvl | ((uint32_t)min(nq, 8) << 6) | ((uint32_t)min(np, 8) << 10) | ((uint32_t)off << 14) |
+           ((uint32_t)p << 27) | ((uint32_t)first << 29) | ((uint32_t)last << 30);
+}
+
+template <int STEP>
+__device__ __forceinline__ void filter_line_class(int cls, uint16_t* q, int step, int nq, int np, const Strength& s,
+                                                  int bd) {
+    if (cls == 0) line_size4<STEP>(q, step, nq, np, s, bd);
+    else if (cls == 1) line_size6<STEP>(q, step, nq, np, s, bd);
+    else if (cls == 2) line_size8<STEP>(q, step, nq, np, s, bd);
+    else line_size16<STEP>(q, step, nq, np, s, bd);
+}
+
+// One deblocking pass over the staged tiles of every plane (PASS 0: vertical
+// edges X = px0 + 4e, e <= tw/4, on 4-row cells from py0-8 (luma) or py0-4
+// (chroma); PASS 1: horizontal edges E = py0 + 4e, e <= th/4, on 4-column
+// cells from px0-4).  Each candidate segment gets its decision (7.14.2-7.14.5:
+// on screen, transform edge, filter size, level) and joins the list of its
+// size class.  The lines are then filtered in one loop over the class lists
+// laid end to end, 4 lanes per segment, so a warp changes filter code at most
+// at a class boundary.  The first and last cell of an edge contribute only
+// the lines the window needs: rows [py0-7, py0+th+7) / [py0-3, py0+th+3) in
+// pass 0, columns [px0-2, px0+tw+2) in pass 1.  Within a pass no two edges
+// touch a common sample, so the lines run in place in any order.
+template <int PASS>
+__device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem, int x0, int y0,
+                                             uint32_t* s_list, int* s_count) {
+    const int tid = threadIdx.x;
+    if (tid < 4) s_count[tid] = 0;
+    __syncthreads();
+    const PlaneGeom gl = plane_geom(0, a.ssx, a.ssy), gc = plane_geom(1, a.ssx, a.ssy);
+    const int na0 = PASS == 0 ? gl.th / 4 + 4 : gl.th / 4 + 1, nb0 = PASS == 0 ? gl.tw / 4 + 1 : gl.tw / 4 + 2;
+    const int nac = PASS == 0 ? gc.th / 4 + 2 : gc.th / 4 + 1, nbc = PASS == 0 ? gc.tw / 4 + 1 : gc.tw / 4 + 2;
+    const int n0 = na0 * nb0, nc = a.num_planes > 1 ? nac * nbc : 0;
+    for (int i = tid; i < n0 + 2 * nc; i += kThreads) {
+        int p = 0, j = i;
+        if (j >= n0) {
+            j -= n0;
+            p = 1;
+            if (j >= nc) {
+                j -= nc;
+                p = 2;
+            }
+        }
+        if (p != 0 && a.levels[1 + p] == 0) continue;
+        const PlaneGeom g = p ? gc : gl;
+        const int na = p ? nac : na0, nb = p ? nbc : nb0;
+        const int ia = j / nb, ib = j - ia * nb;
+        const DevPlane& P = a.dst[p];
+        const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+        const int yp = PASS == 0 ? py0 - (p ? 4 : 8) + 4 * ia : py0 + 4 * ia;
+        const int xp = PASS == 0 ? px0 + 4 * ib : px0 - 4 + 4 * ib;
+        const int col = (xp >> 2) << g.sx, row = (yp >> 2) << g.sy;
+        const bool on_screen = xp >= 0 && yp >= 0 && xp < P.width && yp < P.height && col * 4 < a.coded_width &&
+                               row * 4 < a.coded_height && (PASS == 0 ? xp > 0 : yp > 0);
+        if (!on_screen) continue;
+        const uint8_t* map = p ? a.tx_chroma : a.tx_luma;
+        const int map_cols = p ? (a.mi_cols + a.ssx) >> a.ssx : a.mi_cols;
+        const long cell = (long)(yp >> 2) * map_cols + (xp >> 2);
+        const int cur = map[cell];
+        const int prev = PASS == 0 ? map[cell - 1] : map[cell - map_cols];
+        const int cl = PASS == 0 ? tx_w_log2(cur) : tx_h_log2(cur);
+        const int pl = PASS == 0 ? tx_w_log2(prev) : tx_h_log2(prev);
+        if (((PASS == 0 ? xp : yp) & ((1 << cl) - 1)) != 0) continue;
+        const int size = min(p ? 8 : 16, 1 << min(cl, pl));
+        const int r = row | g.sy, c = col | g.sx;
+        const int li = p == 0 ? PASS : p + 1;  // level index (7.14.5)
+        int lvl;
+        if (a.lvl_map) {
+            lvl = __ldg(a.lvl_map + ((long)r * a.mi_cols + c) * 4 + li);
+            if (lvl == 0) {
+                const int pr = PASS == 0 ? r : r - (1 << g.sy);
+                const int pc = PASS == 0 ? c - (1 << g.sx) : c;
+                lvl = __ldg(a.lvl_map + ((long)pr * a.mi_cols + pc) * 4 + li);
+            }
+        } else {
+            lvl = a.levels[li];
+        }
+        if (lvl == 0) continue;
+        const int cls = size == 4 ? 0 : p ? 1 : size == 8 ? 2 : 3;
+        const int off = (yp - py0 + kHalo) * g.pitch + (xp - px0 + kHalo);
+        const int nq = PASS == 0 ? P.width - xp : P.height - yp, np = PASS == 0 ? xp : yp;
+        const int at = atomicAdd(&s_count[cls], 1);
+        s_list[c_list_off[cls] + at] =
+            seg_entry(lvl, nq, np, off, p, PASS == 0 ? ia == 0 : ib == 0, PASS == 0 ? ia == na - 1 : ib == nb - 1);
+    }
+    __syncthreads();
+    const int c0 = s_count[0], c1 = s_count[1], c2 = s_count[2], c3 = s_count[3];
+    const int lines = 4 * (c0 + c1 + c2 + c3);
+    for (int item = tid; item < lines; item += kThreads) {
+        int seg = item >> 2, cls = 0;
+        const int line = item & 3;
+        if (seg >= c0) {
+            seg -= c0;
+            cls = 1;
+            if (seg >= c1) {
+                seg -= c1;
+                cls = 2;
+                if (seg >= c2) {
+                    seg -= c2;
+                    cls = 3;
+                }
+            }
+        }
+        const uint32_t e = s_list[c_list_off[cls] + seg];
+        const bool first = (e >> 29) & 1, last = (e >> 30) & 1;
+        if (PASS == 0 ? ((first && line == 0) || (last && line == 3)) : ((first && line < 2) || (last && line >= 2)))
+            continue;
+        const int lvl = e & 63, nq = (e >> 6) & 15, np = (e >> 10) & 15, off = (e >> 14) & 0x1FFF, p = (e >> 27) & 3;
+        const int pitch = p ? gc.pitch : gl.pitch;
+        const Strength s = strength_of(lvl, a.sharpness);
+        if (PASS == 0) {
+            filter_line_class<1>(cls, smem + a.plane_off[p] + off + line * pitch, 1, nq, np, s, a.bit_depth);
+        } else {
+            uint16_t* q = smem + a.plane_off[p] + off + line;
+            if (pitch == 64 + 2 * kHalo) filter_line_class<64 + 2 * kHalo>(cls, q, pitch, nq, np, s, a.bit_depth);
+            else filter_line_class<32 + 2 * kHalo>(cls, q, pitch, nq, np, s, a.bit_depth);
+        }
+    }
+    __syncthreads();
 }
 
 // One 64x64 filter block (tile_x, tile_y) of one frame.  Every thread of the
@@ -237,108 +367,9 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     __syncthreads();
 
     // ---- deblocking, pass 0 (vertical edges) then pass 1 (horizontal edges)
-    //
-    // Per pass, every 4-sample edge segment of the needed region gets its
-    // decision (7.14.2-7.14.5: on screen, transform edge, filter size, level)
-    // and is appended to the list of its size class; the lists are then
-    // filtered one class at a time (4 lanes per segment, one per line), so a
-    // warp never mixes the 4-, 6-, 8- and 14-tap code paths.
-    //   pass 0 segments: rows [py0-8, py0+th+8) in 4-row cells x edges
-    //                    X = px0-4+4e, e < tw/4+3
-    //   pass 1 segments: edges E = py0-4+4e, e < th/4+3 x 4-column cells from
-    //                    px0-4, covering columns [px0-2, px0+tw+2)
-    // The horizontal edges read rows [E-7, E+6] only where their filter is
-    // 14 taps (E a multiple of 16), so [py0-7, py0+th+6] bounds every read.
     if (a.deblock_on) {
-        for (int pass = 0; pass < 2; ++pass) {
-            if (tid < 4) s_count[tid] = 0;
-            __syncthreads();
-            for (int p = 0; p < a.num_planes; ++p) {
-                if (p != 0 && a.levels[1 + p] == 0) continue;
-                const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
-                const DevPlane& P = a.dst[p];
-                const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
-                const uint8_t* map = p ? a.tx_chroma : a.tx_luma;
-                const int map_cols = p ? (a.mi_cols + a.ssx) >> a.ssx : a.mi_cols;
-                const int n_a = pass == 0 ? g.th / 4 + 4 : g.th / 4 + 3;
-                const int n_b = pass == 0 ? g.tw / 4 + 3 : g.tw / 4 + 2;
-                for (int i = tid; i < n_a * n_b; i += kThreads) {
-                    const int ia = i / n_b, ib = i - ia * n_b;
-                    const int yp = pass == 0 ? py0 - 8 + 4 * ia : py0 - 4 + 4 * ia;
-                    const int xp = px0 - 4 + 4 * ib;
-                    const int col = (xp >> 2) << g.sx, row = (yp >> 2) << g.sy;
-                    const bool on_screen = xp >= 0 && yp >= 0 && xp < P.width && yp < P.height &&
-                                           col * 4 < a.coded_width && row * 4 < a.coded_height &&
-                                           (pass == 0 ? xp > 0 : yp > 0);
-                    if (!on_screen) continue;
-                    const int cur = map[(long)(yp >> 2) * map_cols + (xp >> 2)];
-                    const int prev = pass == 0 ? map[(long)(yp >> 2) * map_cols + (xp >> 2) - 1]
-                                               : map[(long)((yp >> 2) - 1) * map_cols + (xp >> 2)];
-                    const int cl = pass == 0 ? tx_w_log2(cur) : tx_h_log2(cur);
-                    const int pl = pass == 0 ? tx_w_log2(prev) : tx_h_log2(prev);
-                    if (((pass == 0 ? xp : yp) & ((1 << cl) - 1)) != 0) continue;
-                    const int size = min(p ? 8 : 16, 1 << min(cl, pl));
-                    const int r = row | g.sy, c = col | g.sx;
-                    const int li = p == 0 ? pass : p + 1;  // level index (7.14.5)
-                    int lvl;
-                    if (a.lvl_map) {
-                        lvl = __ldg(a.lvl_map + ((long)r * a.mi_cols + c) * 4 + li);
-                        if (lvl == 0) {
-                            const int pr = pass == 0 ? r : r - (1 << g.sy);
-                            const int pc = pass == 0 ? c - (1 << g.sx) : c;
-                            lvl = __ldg(a.lvl_map + ((long)pr * a.mi_cols + pc) * 4 + li);
-                        }
-                    } else {
-                        lvl = a.levels[li];
-                    }
-                    if (lvl == 0) continue;
-                    const int cls = size == 4 ? 0 : p ? 1 : size == 8 ? 2 : 3;
-                    const int at = atomicAdd(&s_count[cls], 1);
-                    s_list[c_list_off[cls] + at] = (uint32_t)((p << 28) | (i << 8) | lvl);
-                }
-            }
-            __syncthreads();
-            for (int cls = 0; cls < 4; ++cls) {
-                const int count = s_count[cls];
-                for (int item = tid; item < count * 4; item += kThreads) {
-                    const uint32_t e = s_list[c_list_off[cls] + (item >> 2)];
-                    const int line = item & 3, p = e >> 28, i = (e >> 8) & 0xFFFFF, lvl = e & 0xFF;
-                    const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
-                    const DevPlane& P = a.dst[p];
-                    const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
-                    uint16_t* t = smem + a.plane_off[p];
-                    const Strength s = strength_of(lvl, a.sharpness);
-                    if (pass == 0) {
-                        const int n_b = g.tw / 4 + 3;
-                        const int ia = i / n_b, ib = i - ia * n_b;
-                        const int yp = py0 - 8 + 4 * ia + line, xp = px0 - 4 + 4 * ib;
-                        uint16_t* q = t + (yp - py0 + kHalo) * g.pitch + (xp - px0 + kHalo);
-                        const int nq = P.width - xp, np = xp;
-                        if (cls == 0) line_size4<1>(q, 1, nq, np, s, a.bit_depth);
-                        else if (cls == 1) line_size6<1>(q, 1, nq, np, s, a.bit_depth);
-                        else if (cls == 2) line_size8<1>(q, 1, nq, np, s, a.bit_depth);
-                        else line_size16<1>(q, 1, nq, np, s, a.bit_depth);
-                    } else {
-                        const int n_b = g.tw / 4 + 2;
-                        const int ia = i / n_b, ib = i - ia * n_b;
-                        const int yp = py0 - 4 + 4 * ia, xp = px0 - 4 + 4 * ib + line;
-                        if (xp < px0 - 2 || xp >= px0 + g.tw + 2 || xp >= P.width) continue;
-                        uint16_t* q = t + (yp - py0 + kHalo) * g.pitch + (xp - px0 + kHalo);
-                        const int nq = P.height - yp, np = yp;
-                        if (g.pitch == 96) {
-                            if (cls == 0) line_size4<96>(q, 96, nq, np, s, a.bit_depth);
-                            else if (cls == 1) line_size6<96>(q, 96, nq, np, s, a.bit_depth);
-                            else if (cls == 2) line_size8<96>(q, 96, nq, np, s, a.bit_depth);
-                            else line_size16<96>(q, 96, nq, np, s, a.bit_depth);
-                        } else {
-                            if (cls == 0) line_size4<0>(q, g.pitch, nq, np, s, a.bit_depth);
-                            else line_size6<0>(q, g.pitch, nq, np, s, a.bit_depth);
-                        }
-                    }
-                }
-            }
-            __syncthreads();
-        }
+        deblock_pass<0>(a, smem, x0, y0, s_list, s_count);
+        deblock_pass<1>(a, smem, x0, y0, s_list, s_count);
     }
 
     // ---- stripe-boundary rows of the deblocked picture for restoration:
@@ -455,12 +486,13 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
         const bool edge = px0 < 2 || py0 < 2 || px0 + g.tw + 2 > d.width || py0 + g.th + 2 > d.height;
         const uint16_t* tp = smem + a.plane_off[p];
-        if (g.pitch == 96 && g.th == 64) {
-            filter_pairs<96, 8, 1>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
-        } else if (g.pitch == 64 && g.th == 32) {
-            filter_pairs<64, 4, 2>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
+        // tile layouts: 64x64 (luma, 4:4:4 chroma), 32x32 (4:2:0), 32x64 (4:2:2)
+        if (g.tw == 64) {
+            filter_pairs<64 + 2 * kHalo, 8, 1>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
+        } else if (g.th == 32) {
+            filter_pairs<32 + 2 * kHalo, 4, 2>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
         } else {
-            filter_pairs<64, 8, 2>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
+            filter_pairs<32 + 2 * kHalo, 8, 2>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
         }
     }
 }

@@ -242,7 +242,7 @@ extern "C" int32_t vaco_av1_server_open_stream(vaco_av1_server* s, const vaco_av
     const vaco_av1_frame_info& i = *info;
     if (i.mi_rows <= 0 || i.mi_cols <= 0 || i.coded_width <= 0 || i.coded_height <= 0 ||
         i.mi_cols != 2 * ((i.coded_width + 7) >> 3) || i.mi_rows != 2 * ((i.coded_height + 7) >> 3) ||
-        i.upscaled_width < i.coded_width) {
+        i.upscaled_width < i.coded_width || !av1_subsampling_ok(i.subsampling_x, i.subsampling_y)) {
         if (msg) *msg = VACO_AV1_MSG_FRAME_GEOMETRY;
         return VACO_AV1_INVALID_DATA;
     }
