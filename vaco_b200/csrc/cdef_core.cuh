@@ -247,23 +247,41 @@ __device__ __forceinline__ void pair_tap_step(uint32_t v, uint32_t cur, uint32_t
     mx = vmax2(mx, MASK_MAX ? (v & 0x3FFF3FFFu) : v);
 }
 
+// Which tap sets a tile's blocks use.  vaco's filter_block clamps the result
+// to the min/max of every available tap, but when only one tap set has a
+// non-zero strength that clamp never binds: the set's weights sum to 12 <= 16
+// and |constrain(d)| <= |d|, so cur + Round(sum/16) stays inside the taps'
+// range (for sum > 0: (8 + 12 D) >> 4 <= D for every D >= 0, D = max - cur;
+// for sum < 0: (7 - 12 E) >> 4 >= -E, E = cur - min).  A zero strength also
+// makes every constrain() of its set 0.  So the taps of a set whose preset
+// strength is zero are skipped altogether (pri_on / sec_on, uniform over a
+// tile), bit-exactly: the clamp over the remaining set is a no-op.
+
 // Filter the pixel pair whose left sample is at `s` (4-byte aligned).  `taps`
 // are the 12 tap positions of the block for this lane, `row` the word offset
-// of the current row relative to the block's first row.
+// of the current row relative to the block's first row.  MASK_MAX: the tile
+// touches a plane edge, so sentinel samples must not raise the maximum.
 template <bool MASK_MAX>
-__device__ __forceinline__ uint32_t filter_pair(uint32_t cur, const PairTap* taps, int row, const PairBlock& f) {
+__device__ __forceinline__ uint32_t filter_pair(uint32_t cur, const PairTap* taps, int row, const PairBlock& f,
+                                                bool pri_on, bool sec_on) {
     const uint32_t tp = f.pri | ((uint32_t)f.pri << 16), ts = f.sec | ((uint32_t)f.sec << 16);
     const uint32_t pm = (0xFFFFu >> f.pri_shift) * 0x10001u, sm = (0xFFFFu >> f.sec_shift) * 0x10001u;
     uint32_t accp = 0, accn = 0, mn = cur, mx = cur;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const uint32_t wp = k ? f.pt1 : f.pt0, ws = 2 - k;
-        pair_tap_step<MASK_MAX>(load_pair(taps[2 * k], row), cur, tp, f.pri_shift, pm, wp, accp, accn, mn, mx);
-        pair_tap_step<MASK_MAX>(load_pair(taps[2 * k + 1], row), cur, tp, f.pri_shift, pm, wp, accp, accn, mn, mx);
-        pair_tap_step<MASK_MAX>(load_pair(taps[4 + 2 * k], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn, mx);
-        pair_tap_step<MASK_MAX>(load_pair(taps[4 + 2 * k + 1], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn, mx);
-        pair_tap_step<MASK_MAX>(load_pair(taps[8 + 2 * k], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn, mx);
-        pair_tap_step<MASK_MAX>(load_pair(taps[8 + 2 * k + 1], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn, mx);
+        if (pri_on) {
+            pair_tap_step<MASK_MAX>(load_pair(taps[2 * k], row), cur, tp, f.pri_shift, pm, wp, accp, accn, mn, mx);
+            pair_tap_step<MASK_MAX>(load_pair(taps[2 * k + 1], row), cur, tp, f.pri_shift, pm, wp, accp, accn, mn, mx);
+        }
+        if (sec_on) {
+            pair_tap_step<MASK_MAX>(load_pair(taps[4 + 2 * k], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn, mx);
+            pair_tap_step<MASK_MAX>(load_pair(taps[4 + 2 * k + 1], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn,
+                                    mx);
+            pair_tap_step<MASK_MAX>(load_pair(taps[8 + 2 * k], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn, mx);
+            pair_tap_step<MASK_MAX>(load_pair(taps[8 + 2 * k + 1], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn,
+                                    mx);
+        }
     }
     const uint32_t both = vmin2(accp, accn);
     const uint32_t rp = ((accp - both + 0x00080008u) >> 4) & 0x0FFF0FFFu;

@@ -91,10 +91,12 @@ struct DbCdefArgs {
 // CDEF output of one plane tile from the staged (deblocked) samples: warp w
 // filters block row w; lane l owns pixel pairs at tile column 2*(l % ppr),
 // rows l / ppr + RPI*j.  PITCH is the staged pitch, BH the block height.
-template <int PITCH, int BH, int RPI>
+// pri_on / sec_on: the tile preset's primary / secondary strength is
+// non-zero; with neither, every sample stays as it is.
+template <int PITCH, int BH, int RPI, bool EDGE>
 __device__ __forceinline__ void filter_pairs(const uint16_t* t, const DevPlane& d, int px0, int py0, int tw,
-                                             const uint8_t* active, const PairBlock* blocks, bool edge, int warp,
-                                             int lane, int sx) {
+                                             const uint8_t* active, const PairBlock* blocks, bool pri_on, bool sec_on,
+                                             int warp, int lane, int sx) {
     const int ppr = 32 / RPI;              // pairs per row
     const int lp = lane % ppr, lr = lane / ppr;
     const int x = 2 * lp;
@@ -110,7 +112,8 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const DevPlane& 
     const int base_i = (kHalo + r0 + lr) * PITCH + kHalo + x;  // left sample, first row of this lane
     uint32_t* o = reinterpret_cast<uint32_t*>(d.data + (long)(py0 + r0 + lr) * d.stride + gx);
     const long ostride = (long)d.stride * RPI / 2;  // words per RPI rows
-    if (active[b]) {
+    const uint32_t* cw = reinterpret_cast<const uint32_t*>(t + base_i);
+    if ((pri_on || sec_on) && active[b]) {
         const PairBlock f = blocks[b];
         PairTap taps[12];
 #pragma unroll
@@ -118,21 +121,25 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const DevPlane& 
             taps[2 * k] = pair_tap(t, base_i + f.off[k]);
             taps[2 * k + 1] = pair_tap(t, base_i - f.off[k]);
         }
-        const uint32_t* cw = reinterpret_cast<const uint32_t*>(t + base_i);
-#pragma unroll
+#pragma unroll 2
         for (int j = 0; j < BH / RPI; ++j) {
-            const int rr = lr + RPI * j;
             const int woff = j * RPI * PITCH / 2;
-            const uint32_t cur = cw[woff];
-            const uint32_t v = edge ? filter_pair<true>(cur, taps, woff, f) : filter_pair<false>(cur, taps, woff, f);
-            if (col_in && rr < rows_here) o[j * ostride] = v;
+            const uint32_t v = filter_pair<EDGE>(cw[woff], taps, woff, f, pri_on, sec_on);
+            if (col_in && lr + RPI * j < rows_here) o[j * ostride] = v;
         }
     } else if (col_in) {
-        const uint32_t* cw = reinterpret_cast<const uint32_t*>(t + base_i);
 #pragma unroll
         for (int j = 0; j < BH / RPI; ++j)
             if (lr + RPI * j < rows_here) o[j * ostride] = cw[j * RPI * PITCH / 2];
     }
+}
+
+template <int PITCH, int BH, int RPI>
+__device__ __forceinline__ void filter_pairs_edge(bool edge, const uint16_t* t, const DevPlane& d, int px0, int py0,
+                                                  int tw, const uint8_t* active, const PairBlock* blocks, bool pri_on,
+                                                  bool sec_on, int warp, int lane, int sx) {
+    if (edge) filter_pairs<PITCH, BH, RPI, true>(t, d, px0, py0, tw, active, blocks, pri_on, sec_on, warp, lane, sx);
+    else filter_pairs<PITCH, BH, RPI, false>(t, d, px0, py0, tw, active, blocks, pri_on, sec_on, warp, lane, sx);
 }
 
 // Segment-list entry: level (6 bits) | samples on the q side, capped at 8 (4)
@@ -486,13 +493,22 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
         const bool edge = px0 < 2 || py0 < 2 || px0 + g.tw + 2 > d.width || py0 + g.th + 2 > d.height;
         const uint16_t* tp = smem + a.plane_off[p];
+        // the tile's tap sets, from its preset (uniform over the tile)
+        bool pri_on = true, sec_on = true;
+        if (index < 8) {
+            pri_on = (p ? a.uv_pri[index] : a.y_pri[index]) != 0;
+            sec_on = (p ? a.uv_sec[index] : a.y_sec[index]) != 0;
+        }
         // tile layouts: 64x64 (luma, 4:4:4 chroma), 32x32 (4:2:0), 32x64 (4:2:2)
         if (g.tw == 64) {
-            filter_pairs<64 + 2 * kHalo, 8, 1>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
+            filter_pairs_edge<64 + 2 * kHalo, 8, 1>(edge, tp, d, px0, py0, g.tw, s_active, s_pair[p], pri_on, sec_on,
+                                                    warp, lane, g.sx);
         } else if (g.th == 32) {
-            filter_pairs<32 + 2 * kHalo, 4, 2>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
+            filter_pairs_edge<32 + 2 * kHalo, 4, 2>(edge, tp, d, px0, py0, g.tw, s_active, s_pair[p], pri_on, sec_on,
+                                                    warp, lane, g.sx);
         } else {
-            filter_pairs<32 + 2 * kHalo, 8, 2>(tp, d, px0, py0, g.tw, s_active, s_pair[p], edge, warp, lane, g.sx);
+            filter_pairs_edge<32 + 2 * kHalo, 8, 2>(edge, tp, d, px0, py0, g.tw, s_active, s_pair[p], pri_on, sec_on,
+                                                    warp, lane, g.sx);
         }
     }
 }
