@@ -18,10 +18,31 @@ constexpr int kSent = 0xC000;      // > any 12-bit sample; & kMaxMask == 0
 constexpr int kMaxMask = 0x3FFF;
 
 // (row, col) step per direction and distance (src/cdef.rs:57-66).
-__constant__ int8_t c_dir[8][2][2] = {
+struct DirTable {
+    int8_t v[8][2][2];
+};
+constexpr DirTable kDir = {{
     {{-1, 1}, {-2, 2}}, {{0, 1}, {-1, 2}}, {{0, 1}, {0, 2}},  {{0, 1}, {1, 2}},
     {{1, 1}, {2, 2}},   {{1, 0}, {2, 1}},  {{1, 0}, {2, 0}},  {{1, 0}, {2, -1}},
-};
+}};
+// The table packed into one 24-bit immediate per (distance, axis): 3 bits
+// per direction, biased by 2.  A lookup with a per-lane direction is then a
+// shift and a mask instead of a divergent constant-memory read.
+__host__ __device__ constexpr uint32_t dir_packed(int k, int axis) {
+    uint32_t m = 0;
+    for (int d = 0; d < 8; ++d) m |= (uint32_t)(kDir.v[d][k][axis] + 2) << (3 * d);
+    return m;
+}
+template <int K, int AXIS>
+__device__ __forceinline__ int dir_step(int d) {
+    constexpr uint32_t m = dir_packed(K, AXIS);
+    return (int)((m >> (3 * d)) & 7u) - 2;
+}
+// Sample offset of tap distance K along direction d in a plane of `pitch`.
+template <int K>
+__device__ __forceinline__ int dir_offset(int d, int pitch) {
+    return dir_step<K, 0>(d) * pitch + dir_step<K, 1>(d);
+}
 
 // Line index of pixel (i, j) for direction d (src/cdef.rs:88-97).
 __host__ __device__ constexpr int dir_bin(int d, int i, int j) {
@@ -120,12 +141,12 @@ struct BlockFilter {
 
 __device__ __forceinline__ BlockFilter make_filter(int dir, int pri, int sec, int damping, int shift, int pitch) {
     BlockFilter f;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        f.off[k] = c_dir[dir][k][0] * pitch + c_dir[dir][k][1];
-        f.off[2 + k] = c_dir[(dir + 2) & 7][k][0] * pitch + c_dir[(dir + 2) & 7][k][1];
-        f.off[4 + k] = c_dir[(dir + 6) & 7][k][0] * pitch + c_dir[(dir + 6) & 7][k][1];
-    }
+    f.off[0] = dir_offset<0>(dir, pitch);
+    f.off[1] = dir_offset<1>(dir, pitch);
+    f.off[2] = dir_offset<0>((dir + 2) & 7, pitch);
+    f.off[3] = dir_offset<1>((dir + 2) & 7, pitch);
+    f.off[4] = dir_offset<0>((dir + 6) & 7, pitch);
+    f.off[5] = dir_offset<1>((dir + 6) & 7, pitch);
     f.pri = (short)pri;
     f.sec = (short)sec;
     f.pri_shift = (uint8_t)(pri ? max(0, damping - ilog2u(pri)) : 0);
@@ -198,12 +219,12 @@ struct PairBlock {
 
 __device__ __forceinline__ PairBlock make_pair_block(int dir, int pri, int sec, int damping, int shift, int pitch) {
     PairBlock f;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        f.off[k] = (int16_t)(c_dir[dir][k][0] * pitch + c_dir[dir][k][1]);
-        f.off[2 + k] = (int16_t)(c_dir[(dir + 2) & 7][k][0] * pitch + c_dir[(dir + 2) & 7][k][1]);
-        f.off[4 + k] = (int16_t)(c_dir[(dir + 6) & 7][k][0] * pitch + c_dir[(dir + 6) & 7][k][1]);
-    }
+    f.off[0] = (int16_t)dir_offset<0>(dir, pitch);
+    f.off[1] = (int16_t)dir_offset<1>(dir, pitch);
+    f.off[2] = (int16_t)dir_offset<0>((dir + 2) & 7, pitch);
+    f.off[3] = (int16_t)dir_offset<1>((dir + 2) & 7, pitch);
+    f.off[4] = (int16_t)dir_offset<0>((dir + 6) & 7, pitch);
+    f.off[5] = (int16_t)dir_offset<1>((dir + 6) & 7, pitch);
     f.pri = (uint16_t)pri;
     f.sec = (uint16_t)sec;
     f.pri_shift = (uint8_t)(pri ? max(0, damping - ilog2u(pri)) : 0);

@@ -46,6 +46,18 @@ constexpr int kHalo = 8;
 __constant__ int c_list_off[4] = {0, 1020, 1700, 2040};
 constexpr int kListTotal = 2380;
 
+// Side-information window of a tile: cells [mi_r0 - kWinTop, +kWinRows) x
+// [mi_c0 - kWinLeft, +kWinCols) of the luma maps, and the same shape around
+// the tile's own cell origin in the chroma transform map.  Relative to the
+// tile, the two passes read transform sizes at cell rows [-2, 17] and
+// columns [-1, 16] (previous cells included), and subsampled chroma reads
+// levels at luma cells up to row and column 17.
+constexpr int kWinTop = 3, kWinLeft = 2, kWinRows = 22, kWinCols = 20, kWinCells = kWinRows * kWinCols;
+struct SideWindow {
+    uint8_t tx[2][kWinCells];  // luma, chroma TX_SIZE
+    uint32_t lvl[kWinCells];   // loop-filter levels (Yv, Yh, U, V) when a level map is given
+};
+
 struct PlaneGeom {
     int tw, th;        // tile extent in this plane
     int pitch, rows;   // staged region
@@ -174,7 +186,7 @@ __device__ __forceinline__ void filter_line_class(int cls, uint16_t* q, int step
 // touch a common sample, so the lines run in place in any order.
 template <int PASS>
 __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem, int x0, int y0,
-                                             uint32_t* s_list, int* s_count) {
+                                             const SideWindow& side, uint32_t* s_list, int* s_count) {
     const int tid = threadIdx.x;
     if (tid < 4) s_count[tid] = 0;
     __syncthreads();
@@ -204,11 +216,10 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
         const bool on_screen = xp >= 0 && yp >= 0 && xp < P.width && yp < P.height && col * 4 < a.coded_width &&
                                row * 4 < a.coded_height && (PASS == 0 ? xp > 0 : yp > 0);
         if (!on_screen) continue;
-        const uint8_t* map = p ? a.tx_chroma : a.tx_luma;
-        const int map_cols = p ? (a.mi_cols + a.ssx) >> a.ssx : a.mi_cols;
-        const long cell = (long)(yp >> 2) * map_cols + (xp >> 2);
-        const int cur = map[cell];
-        const int prev = PASS == 0 ? map[cell - 1] : map[cell - map_cols];
+        const uint8_t* map = side.tx[p ? 1 : 0];
+        const int w = ((yp - py0) / 4 + kWinTop) * kWinCols + (xp - px0) / 4 + kWinLeft;
+        const int cur = map[w];
+        const int prev = PASS == 0 ? map[w - 1] : map[w - kWinCols];
         const int cl = PASS == 0 ? tx_w_log2(cur) : tx_h_log2(cur);
         const int pl = PASS == 0 ? tx_w_log2(prev) : tx_h_log2(prev);
         if (((PASS == 0 ? xp : yp) & ((1 << cl) - 1)) != 0) continue;
@@ -217,11 +228,12 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
         const int li = p == 0 ? PASS : p + 1;  // level index (7.14.5)
         int lvl;
         if (a.lvl_map) {
-            lvl = __ldg(a.lvl_map + ((long)r * a.mi_cols + c) * 4 + li);
+            const int mi_r0 = y0 >> 2, mi_c0 = x0 >> 2;
+            const int lw = (r - mi_r0 + kWinTop) * kWinCols + c - mi_c0 + kWinLeft;
+            lvl = (side.lvl[lw] >> (8 * li)) & 0xFF;
             if (lvl == 0) {
-                const int pr = PASS == 0 ? r : r - (1 << g.sy);
-                const int pc = PASS == 0 ? c - (1 << g.sx) : c;
-                lvl = __ldg(a.lvl_map + ((long)pr * a.mi_cols + pc) * 4 + li);
+                const int pw = PASS == 0 ? lw - (1 << g.sx) : lw - (kWinCols << g.sy);
+                lvl = (side.lvl[pw] >> (8 * li)) & 0xFF;
             }
         } else {
             lvl = a.levels[li];
@@ -278,9 +290,9 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     __shared__ int s_cost[64][8];
     __shared__ PairBlock s_pair[3][64];
     __shared__ uint8_t s_active[64];
-    __shared__ uint32_t s_list[kListTotal];  // per size class: plane<<28 | segment<<8 | level
+    __shared__ uint32_t s_list[kListTotal];  // per size class, see seg_entry()
     __shared__ int s_count[4];
-    __shared__ int s_any, s_bad;
+    __shared__ SideWindow s_side;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int mi_r0 = tile_y * 16, mi_c0 = tile_x * 16;
@@ -290,14 +302,9 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     // ---- CDEF block activity (decode.rs:772-779)
     const long slot = (long)(mi_r0 >> 4) * a.cdef_stride + (mi_c0 >> 4);
     const int index = (a.cdef_on && slot < a.cdef_count) ? __ldg(a.cdef_idx + slot) : -1;
-    if (tid == 0) {
-        s_any = 0;
-        s_bad = 0;
-    }
-    __syncthreads();
+    bool act = false;
     if (tid < 64) {
         const int r = mi_r0 + (tid >> 3) * 2, c = mi_c0 + (tid & 7) * 2;
-        bool act = false;
         if (r < a.mi_rows && c < a.mi_cols && index >= 0) {
             auto sk = [&](int rr, int cc) {
                 return rr < a.mi_rows && cc < a.mi_cols && a.skip[(long)rr * a.mi_cols + cc] != 0;
@@ -305,20 +312,67 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
             act = !(sk(r, c) && sk(r + 1, c) && sk(r, c + 1) && sk(r + 1, c + 1));
         }
         s_active[tid] = act;
-        if (act) s_any = 1;
     }
 
-    // ---- deblocking side-information checks for this tile's own cells
+    // ---- every plane's tile with an 8-sample halo (edge-clamped).  Whole
+    // 16-byte chunks inside the plane go by cp.async, all in flight at once;
+    // chunks that straddle the left/right plane edge are gathered sample by
+    // sample.  Rows past the top/bottom edge repeat the edge row.
+    for (int p = 0; p < a.num_planes; ++p) {
+        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        const DevPlaneC& P = a.src[p];
+        uint16_t* t = smem + a.plane_off[p];
+        const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+        const int vpr = g.pitch / 8;
+        for (int v = tid; v < g.rows * vpr; v += kThreads) {
+            const int r = v / vpr, cv = v - r * vpr;
+            const int y = clampi(py0 - kHalo + r, 0, P.height - 1);
+            const int x = px0 - kHalo + cv * 8;
+            const uint16_t* row = P.data + (long)y * P.stride;
+            uint16_t* d = t + r * g.pitch + cv * 8;
+            if (a.vec_ok && x >= 0 && x + 8 <= P.width) {
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(d);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(row + x) : "memory");
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) d[k] = __ldg(row + clampi(x + k, 0, P.width - 1));
+            }
+        }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+
+    // ---- the side information the deblocking decisions read, while the
+    // copies are in flight (cells the two passes touch; see SideWindow)
+    {
+        const int crows = (a.mi_rows + a.ssy) >> a.ssy, ccols = (a.mi_cols + a.ssx) >> a.ssx;
+        const int cr0 = (mi_r0 >> a.ssy) - kWinTop, cc0 = (mi_c0 >> a.ssx) - kWinLeft;
+        for (int i = tid; i < kWinCells; i += kThreads) {
+            const int wr = i / kWinCols, wc = i - wr * kWinCols;
+            const int r = mi_r0 - kWinTop + wr, c = mi_c0 - kWinLeft + wc;
+            if (r >= 0 && c >= 0 && r < a.mi_rows && c < a.mi_cols) {
+                const long cell = (long)r * a.mi_cols + c;
+                s_side.tx[0][i] = __ldg(a.tx_luma + cell);
+                if (a.lvl_map) s_side.lvl[i] = __ldg(reinterpret_cast<const uint32_t*>(a.lvl_map) + cell);
+            }
+            if (a.num_planes > 1 && cr0 + wr >= 0 && cc0 + wc >= 0 && cr0 + wr < crows && cc0 + wc < ccols)
+                s_side.tx[1][i] = __ldg(a.tx_chroma + (long)(cr0 + wr) * ccols + cc0 + wc);
+        }
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    const bool any_active = __syncthreads_or(act);
+
+    // ---- input checks from shared memory: the tile's own cells (transform
+    // sizes, levels) and the tile's own samples
     {
         int bad = 0;
         for (int i = tid; i < 256; i += kThreads) {
             const int r = mi_r0 + (i >> 4), c = mi_c0 + (i & 15);
             if (r < a.mi_rows && c < a.mi_cols) {
-                const long cell = (long)r * a.mi_cols + c;
-                bad |= __ldg(a.tx_luma + cell) > 18;
+                const int w = (i >> 4) + kWinTop, wc = (i & 15) + kWinLeft;
+                bad |= s_side.tx[0][w * kWinCols + wc] > 18;
                 if (a.lvl_map) {
-                    const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(a.lvl_map) + cell);
-                    bad |= ((w & 0xFF) > 63) | (((w >> 8) & 0xFF) > 63) | (((w >> 16) & 0xFF) > 63) | ((w >> 24) > 63);
+                    const uint32_t v = s_side.lvl[w * kWinCols + wc];
+                    bad |= ((v & 0xFF) > 63) | (((v >> 8) & 0xFF) > 63) | (((v >> 16) & 0xFF) > 63) | ((v >> 24) > 63);
                 }
             }
         }
@@ -326,57 +380,42 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
             const int ccols = (a.mi_cols + a.ssx) >> a.ssx, crows = (a.mi_rows + a.ssy) >> a.ssy;
             const int cw = 16 >> a.ssx, ch = 16 >> a.ssy;
             for (int i = tid; i < cw * ch; i += kThreads) {
-                const int r = (mi_r0 >> a.ssy) + i / cw, c = (mi_c0 >> a.ssx) + i % cw;
-                if (r < crows && c < ccols) bad |= __ldg(a.tx_chroma + (long)r * ccols + c) > 18;
+                const int dr = i / cw, dc = i - dr * cw;
+                const int r = (mi_r0 >> a.ssy) + dr, c = (mi_c0 >> a.ssx) + dc;
+                if (r < crows && c < ccols) bad |= s_side.tx[1][(dr + kWinTop) * kWinCols + dc + kWinLeft] > 18;
             }
         }
         if (bad) report_error(a.status, STAGE_DEBLOCK, 0, VACO_AV1_MSG_DB_PARAMS);
     }
-
-    // ---- stage every plane with a 16-sample halo (edge-clamped) and check samples
     {
+        const uint32_t hi = ((0xFFFFu << a.bit_depth) & 0xFFFFu) * 0x10001u;  // bits above the depth, per lane
         int bad = 0;
         for (int p = 0; p < a.num_planes; ++p) {
             const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
             const DevPlaneC& P = a.src[p];
-            uint16_t* t = smem + a.plane_off[p];
             const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
-            const int vpr = g.pitch / 8;
-            for (int v = tid; v < g.rows * vpr; v += kThreads) {
-                const int r = v / vpr, cv = v - r * vpr;
-                const int y = clampi(py0 - kHalo + r, 0, P.height - 1);
-                const int x = px0 - kHalo + cv * 8;
-                const bool interior_row = (py0 - kHalo + r) == y && y >= py0 && y < py0 + g.th;
-                const uint16_t* row = P.data + (long)y * P.stride;
-                uint16_t* d = t + r * g.pitch + cv * 8;
-                if (a.vec_ok && x >= 0 && x + 8 <= P.width) {
-                    const uint4 q = __ldg(reinterpret_cast<const uint4*>(row + x));
-                    *reinterpret_cast<uint4*>(d) = q;
-                    if (interior_row && x >= px0 && x < px0 + g.tw) {
-                        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-                        for (int k = 0; k < 4; ++k)
-                            bad |= ((int)(w[k] & 0xFFFF) > maxv) | ((int)(w[k] >> 16) > maxv);
-                    }
+            const int cpr = g.tw / 8, rows = min(g.th, P.height - py0);
+            const uint16_t* t = smem + a.plane_off[p];
+            for (int v = tid; v < rows * cpr; v += kThreads) {
+                const int r = v / cpr, cv = v - r * cpr;
+                const int x = px0 + cv * 8;
+                if (x >= P.width) continue;
+                const uint16_t* q = t + (r + kHalo) * g.pitch + kHalo + cv * 8;
+                if (x + 8 <= P.width) {
+                    const uint4 w = *reinterpret_cast<const uint4*>(q);
+                    bad |= ((w.x | w.y | w.z | w.w) & hi) != 0;
                 } else {
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const int xx = x + k;
-                        const int s = __ldg(row + clampi(xx, 0, P.width - 1));
-                        d[k] = (uint16_t)s;
-                        if (interior_row && xx >= px0 && xx < px0 + g.tw && xx < P.width) bad |= s > maxv;
-                    }
+                    for (int k = 0; k < P.width - x; ++k) bad |= q[k] > maxv;
                 }
             }
         }
         if (bad) report_error(a.status, STAGE_DEBLOCK, 1, VACO_AV1_MSG_DB_SAMPLE);
     }
-    __syncthreads();
 
     // ---- deblocking, pass 0 (vertical edges) then pass 1 (horizontal edges)
     if (a.deblock_on) {
-        deblock_pass<0>(a, smem, x0, y0, s_list, s_count);
-        deblock_pass<1>(a, smem, x0, y0, s_list, s_count);
+        deblock_pass<0>(a, smem, x0, y0, s_side, s_list, s_count);
+        deblock_pass<1>(a, smem, x0, y0, s_side, s_list, s_count);
     }
 
     // ---- stripe-boundary rows of the deblocked picture for restoration:
@@ -404,7 +443,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     }
 
     // ---- CDEF on the deblocked tile
-    if (!s_any) {
+    if (!any_active) {
         // Nothing filtered (or CDEF off): the output is the deblocked tile.
         for (int p = 0; p < a.num_planes; ++p) {
             const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
@@ -451,37 +490,32 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         }
     }
     __syncthreads();
-    if (tid < 64 && s_active[tid]) {
-        const int b = tid;
+    // Per block and plane (one thread each): direction, strengths, checks.
+    if (tid < 64 * a.num_planes && s_active[tid & 63]) {
+        const int b = tid & 63, p = tid >> 6;
         int dir;
         uint32_t var;
         best_direction(s_cost[b], dir, var);
-        bool bad = false;
-        int bad_plane = 0, bad_msg = 0;
-        for (int p = 0; p < a.num_planes; ++p) {
-            const bool chroma = p != 0;
-            int sp = 0, ss = 0;
-            if (index < 8) {
-                sp = chroma ? a.uv_pri[index] : a.y_pri[index];
-                ss = chroma ? a.uv_sec[index] : a.y_sec[index];
-            }
-            int primary = (sp << a.shift) & 0xFFFF;
-            const int secondary = (ss << a.shift) & 0xFFFF;
-            const int chosen = primary == 0 ? 0 : chroma ? chroma_direction(dir, a.ssx, a.ssy) : dir;
-            if (!chroma) primary = adjust_strength(primary, var);
-            const int damping = (a.damping + a.shift - (chroma ? 1 : 0)) & 0xFF;
-            if (!bad && (index >= 8 || damping > 12 || primary > (15 << a.shift) || secondary > (4 << a.shift))) {
-                bad = true;
-                bad_plane = p;
-                bad_msg = index >= 8 ? VACO_AV1_MSG_CDEF_STRENGTH_INDEX : VACO_AV1_MSG_CDEF_BLOCK_PARAMS;
-            }
-            const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
-            s_pair[p][b] = make_pair_block(chosen, primary, secondary, min(damping, 12), a.shift, g.pitch);
+        const bool chroma = p != 0;
+        int sp = 0, ss = 0;
+        if (index < 8) {
+            sp = chroma ? a.uv_pri[index] : a.y_pri[index];
+            ss = chroma ? a.uv_sec[index] : a.y_sec[index];
         }
-        if (bad) {
+        int primary = (sp << a.shift) & 0xFFFF;
+        const int secondary = (ss << a.shift) & 0xFFFF;
+        const int chosen = primary == 0 ? 0 : chroma ? chroma_direction(dir, a.ssx, a.ssy) : dir;
+        if (!chroma) primary = adjust_strength(primary, var);
+        const int damping = (a.damping + a.shift - (chroma ? 1 : 0)) & 0xFF;
+        // Each plane reports its own failure; the status word keeps the
+        // lowest (block, plane) key, i.e. the first plane vaco would reject.
+        if (index >= 8 || damping > 12 || primary > (15 << a.shift) || secondary > (4 << a.shift)) {
             const int r = mi_r0 + (b >> 3) * 2, c = mi_c0 + (b & 7) * 2;
-            report_error(a.status, STAGE_CDEF, ((unsigned long long)r * a.mi_cols + c) * 4 + 1 + bad_plane, bad_msg);
+            report_error(a.status, STAGE_CDEF, ((unsigned long long)r * a.mi_cols + c) * 4 + 1 + p,
+                         index >= 8 ? VACO_AV1_MSG_CDEF_STRENGTH_INDEX : VACO_AV1_MSG_CDEF_BLOCK_PARAMS);
         }
+        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        s_pair[p][b] = make_pair_block(chosen, primary, secondary, min(damping, 12), a.shift, g.pitch);
     }
     __syncthreads();
 
