@@ -168,17 +168,37 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     const int bd = a.bit_depth, maxv = (1 << bd) - 1;
 
     if (P.copy_only || (u.type != VACO_AV1_LR_WIENER && u.type != VACO_AV1_LR_SGRPROJ)) {
-        // RestorationUnit::None: the CDEF output, restoration.rs:194.
-        for (int k = warp; k < R; k += kWarps) {
-            const uint16_t* src = P.after.data + (long)(y_lo + k) * P.after.stride + x_lo;
-            uint16_t* dst = P.out.data + (long)(y_lo + k) * P.out.stride + x_lo;
-            for (int c = lane; c < C; c += 32) dst[c] = src[c];
+        // RestorationUnit::None: the CDEF output, restoration.rs:194.  The
+        // tile is at most 64 x 64 samples = 512 16-byte vectors, so each
+        // thread has both of its loads in flight before it stores.
+        const bool vec = ((P.after.stride | P.out.stride) & 7) == 0 &&
+                         ((reinterpret_cast<uintptr_t>(P.after.data) | reinterpret_cast<uintptr_t>(P.out.data)) & 15) == 0;
+        const int vpr = (C + 7) >> 3;
+        uint4 q[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int i = tid + j * kLrThreads, r = i / vpr, x = x_lo + 8 * (i - r * vpr);
+            if (vec && i < R * vpr && x + 8 <= x_hi)
+                q[j] = __ldg(reinterpret_cast<const uint4*>(P.after.data + (long)(y_lo + r) * P.after.stride + x));
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int i = tid + j * kLrThreads, r = i / vpr, x = x_lo + 8 * (i - r * vpr);
+            if (i >= R * vpr) continue;
+            uint16_t* dst = P.out.data + (long)(y_lo + r) * P.out.stride + x;
+            if (vec && x + 8 <= x_hi) {
+                *reinterpret_cast<uint4*>(dst) = q[j];
+            } else {
+                const uint16_t* src = P.after.data + (long)(y_lo + r) * P.after.stride + x;
+                for (int k = 0; k < min(8, x_hi - x); ++k) dst[k] = src[k];
+            }
         }
         return;
     }
 
     // Stage Source::get (restoration.rs:233-244): rows y_lo-3 .. y_hi+2,
-    // columns x_lo-8 .. x_lo+72 as 10 aligned 8-sample vectors per row.
+    // columns x_lo-8 .. x_lo+72 as 10 aligned 8-sample vectors per row, all
+    // in flight at once by cp.async (edge vectors are gathered sample by sample).
     const int stripe = (y_lo + off) / sh;
     const int s_start = stripe * sh - off, s_end = s_start + sh - 1;
     const int srows = R + 6;
@@ -202,12 +222,14 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
         const int x = x_lo - kSOff + 8 * v;
         uint16_t* d = S + r * kSPitch + 8 * v;
         if (vec_ok && x >= 0 && x + 8 <= P.width) {
-            *reinterpret_cast<uint4*>(d) = __ldg(reinterpret_cast<const uint4*>(row + x));
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(d);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(row + x) : "memory");
         } else {
 #pragma unroll
             for (int k = 0; k < 8; ++k) d[k] = __ldg(row + clampi(x + k, 0, P.width - 1));
         }
     }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
     __syncthreads();
 
     if (u.type == VACO_AV1_LR_WIENER) {
