@@ -60,14 +60,24 @@ struct LrArgs {
 // Shared-memory layout (dynamic):
 //   S      kSRows x kSPitch uint16        staged Source::get values
 //   region either H  kSRows x kMaxTile int16   (Wiener horizontal pass)
-//          or     A  kBox x kBox uint16, B  kBox x kBox int32 (one self-guided pass)
+//          or     A0 kBox0 x kBox uint16, B0 kBox0 x kBox int32 (radius-2 pass,
+//                 box rows of odd y only) and A1 kBox x kBox uint16,
+//                 B1 kBox x kBox int32 (radius-1 pass)
 //   a2tab  256 uint16
+//   V      per warp: 2 x kVCols int32   vertical box sums (sum, sum of squares)
+constexpr int kVCols = kBox + 4 + 2;     // vertical box sums per row: box columns + 2*radius (even)
+constexpr int kBox0 = kBox / 2 + 1;      // radius-2 box rows (odd y only)
+constexpr size_t align16(size_t b) { return (b + 15) / 16 * 16; }
 constexpr size_t kSBytes = sizeof(uint16_t) * kSRows * kSPitch;
-constexpr size_t kABytes = (sizeof(uint16_t) * kBox * kBox + 15) / 16 * 16;
-constexpr size_t kBBytes = sizeof(int32_t) * kBox * kBox;
+constexpr size_t kA0Bytes = align16(sizeof(uint16_t) * kBox0 * kBox);
+constexpr size_t kB0Bytes = sizeof(int32_t) * kBox0 * kBox;
+constexpr size_t kA1Bytes = align16(sizeof(uint16_t) * kBox * kBox);
+constexpr size_t kB1Bytes = sizeof(int32_t) * kBox * kBox;
+constexpr size_t kSgrBytes = kA0Bytes + kB0Bytes + kA1Bytes + kB1Bytes;
 constexpr size_t kHBytes = sizeof(int16_t) * kSRows * kMaxTile;
-constexpr size_t kRegion = (kABytes + kBBytes) > kHBytes ? (kABytes + kBBytes) : kHBytes;
-constexpr size_t kLrSmem = kSBytes + kRegion + 256 * sizeof(uint16_t);
+constexpr size_t kRegion = kSgrBytes > kHBytes ? kSgrBytes : kHBytes;
+constexpr size_t kVBytes = sizeof(int32_t) * 2 * kVCols * kWarps;
+constexpr size_t kLrSmem = kSBytes + kRegion + 256 * sizeof(uint16_t) + kVBytes;
 
 __device__ __forceinline__ int round2i(int v, int s) { return s == 0 ? v : (v + (1 << (s - 1))) >> s; }
 
@@ -87,41 +97,58 @@ __device__ __forceinline__ bool unit_ok(const vaco_av1_lr_unit& u) {
 }
 
 
-// Box sums around every position of one row band and the a2 / b terms of
-// box_ab (restoration.rs:314-339).
+// Box sums around every box position (br, bc) -- box rows y_lo-1+br (only
+// those of odd y when odd_rows_only), box columns x_lo-1+bc -- and the a2 / b
+// terms of box_ab (restoration.rs:314-339).  A warp takes whole box rows:
+// its lanes first form the (2 RAD + 1)-row vertical sums (and sums of
+// squares) of every column the row's boxes reach, in the warp's own buffer
+// V, then each box sum as 2 RAD + 1 of those -- 2 (2 RAD + 1) loads per box
+// instead of (2 RAD + 1)^2.
 template <int RAD>
 __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_t* __restrict__ A,
-                                         int32_t* __restrict__ B, const uint16_t* __restrict__ a2tab, int R, int C,
-                                         int y_lo, bool odd_rows_only, int bd, unsigned scale) {
+                                         int32_t* __restrict__ B, const uint16_t* __restrict__ a2tab,
+                                         int32_t* __restrict__ V, int R, int C, int y_lo, bool odd_rows_only, int bd,
+                                         unsigned scale) {
     constexpr int n = (2 * RAD + 1) * (2 * RAD + 1);
     constexpr unsigned recip = ((1 << 12) + n / 2) / n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int rows = R + 2, cols = C + 2;
     const int sh2 = 2 * (bd - 8), sh1 = bd - 8;
-    // First box row whose y (= y_lo - 1 + br) is odd, when only odd rows are used.
-    const int br0 = odd_rows_only ? ((y_lo - 1) & 1 ? 0 : 1) : 0;
+    // Box rows of odd y (= y_lo - 1 + br) are the even br: tiles start on
+    // even rows (stripe and unit boundaries are even).
     const int rstep = odd_rows_only ? 2 : 1;
-    for (int br = br0 + warp * rstep; br < rows; br += kWarps * rstep) {
+    for (int br = warp * rstep; br < rows; br += kWarps * rstep) {
         // staged row of box row br is br + 2 (box rows start at y0-1, staged at y0-3)
         const uint16_t* srow = S + (br + 2 - RAD) * kSPitch + (kSOff - 1 - RAD);
+        __syncwarp();  // the previous row's sums are consumed
+        for (int cc = lane; cc < cols + 2 * RAD; cc += 32) {
+            int s = 0, q = 0;
+#pragma unroll
+            for (int dy = 0; dy <= 2 * RAD; ++dy) {
+                const int v = srow[dy * kSPitch + cc];
+                s += v;
+                q += v * v;
+            }
+            V[cc] = s;
+            V[kVCols + cc] = q;
+        }
+        __syncwarp();
         for (int bc = lane; bc < cols; bc += 32) {
             int sum = 0, sum_sq = 0;
 #pragma unroll
-            for (int dy = 0; dy <= 2 * RAD; ++dy)
-#pragma unroll
-                for (int dx = 0; dx <= 2 * RAD; ++dx) {
-                    int v = srow[dy * kSPitch + bc + dx];
-                    sum += v;
-                    sum_sq += v * v;
-                }
+            for (int dx = 0; dx <= 2 * RAD; ++dx) {
+                sum += V[bc + dx];
+                sum_sq += V[kVCols + bc + dx];
+            }
             int aa = round2i(sum_sq, sh2);
             int d = round2i(sum, sh1);
             int p = max(aa * n - d * d, 0);
             unsigned long long zz = ((unsigned long long)(unsigned)p * scale + (1u << 19)) >> 20;
             int a2 = a2tab[zz > 255 ? 255 : (int)zz];
             unsigned b = ((unsigned)(256 - a2) * (unsigned)sum * recip + (1u << 11)) >> 12;
-            A[br * kBox + bc] = (uint16_t)a2;
-            B[br * kBox + bc] = (int)b;
+            const int ar = odd_rows_only ? br >> 1 : br;  // odd-only rows are stored compactly
+            A[ar * kBox + bc] = (uint16_t)a2;
+            B[ar * kBox + bc] = (int)b;
         }
     }
 }
@@ -132,9 +159,13 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     uint16_t* S = reinterpret_cast<uint16_t*>(smem_raw);
     unsigned char* region = smem_raw + kSBytes;
     int16_t* H = reinterpret_cast<int16_t*>(region);
-    uint16_t* A = reinterpret_cast<uint16_t*>(region);
-    int32_t* B = reinterpret_cast<int32_t*>(region + kABytes);
+    uint16_t* A0 = reinterpret_cast<uint16_t*>(region);
+    int32_t* B0 = reinterpret_cast<int32_t*>(region + kA0Bytes);
+    uint16_t* A1 = reinterpret_cast<uint16_t*>(region + kA0Bytes + kB0Bytes);
+    int32_t* B1 = reinterpret_cast<int32_t*>(region + kA0Bytes + kB0Bytes + kA1Bytes);
     uint16_t* a2tab = reinterpret_cast<uint16_t*>(region + kRegion);
+    int32_t* Vw = reinterpret_cast<int32_t*>(region + kRegion + 256 * sizeof(uint16_t)) +
+                  (threadIdx.x >> 5) * 2 * kVCols;  // this warp's vertical sums
 
     int pl = 0;
     while (pl + 1 < a.count && block >= a.tile_base[pl + 1]) ++pl;
@@ -254,13 +285,22 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
             }
         }
         __syncthreads();
-        for (int k = warp; k < R; k += kWarps) {
-            uint16_t* dst = P.out.data + (long)(y_lo + k) * P.out.stride + x_lo;
-            for (int c = lane; c < C; c += 32) {
+        // Vertical pass: each thread walks rows 8 warp .. 8 warp + 7 of its
+        // columns, reading each intermediate row once.
+        const int k0 = 8 * warp;
+        if (k0 >= R) return;
+        for (int c = lane; c < C; c += 32) {
+            int h[14];
+#pragma unroll
+            for (int t = 0; t < 14; ++t) h[t] = H[min(k0 + t, kSRows - 1) * kMaxTile + c];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (k0 + j >= R) break;
                 int sum = 0;
 #pragma unroll
-                for (int t = 0; t < 7; ++t) sum += vv[t] * H[(k + t) * kMaxTile + c];
-                dst[c] = (uint16_t)clampi(round2i(sum, 14 - round_h), 0, maxv);
+                for (int t = 0; t < 7; ++t) sum += vv[t] * h[j + t];
+                P.out.data[(long)(y_lo + k0 + j) * P.out.stride + x_lo + c] =
+                    (uint16_t)clampi(round2i(sum, 14 - round_h), 0, maxv);
             }
         }
         return;
@@ -272,61 +312,82 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     const int e0 = c_sgr_e[set][0], e1 = c_sgr_e[set][1];
     for (int z = tid; z < 256; z += kLrThreads)
         a2tab[z] = (uint16_t)(z >= 255 ? 256 : z == 0 ? 1 : ((z << 8) + z / 2) / (z + 1));
-    // Pixel (k, c) of this thread: k = warp + 8*j, c = lane + 32*q.
-    int first[kPix];
+    // Both box passes, into their own buffers, then one final pass.
+    __syncthreads();  // a2tab
     if (r0 != 0) {
         const int n2e = 25 * 25 * e0;
-        __syncthreads();  // a2tab
-        box_pass<2>(S, A, B, a2tab, R, C, y_lo, true, bd, (unsigned)(((1 << 20) + n2e / 2) / n2e));
-        __syncthreads();
-#pragma unroll
-        for (int j = 0; j < kPix / 2; ++j)
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const int k = warp + kWarps * j, c = lane + 32 * q;
-                if (k >= R || c >= C) continue;
-                const int y = y_lo + k;
-                const int orig = S[(k + 3) * kSPitch + kSOff + c];
-                const int bi = (k + 1) * kBox + (c + 1);
-                if (y & 1) {  // weights 6 (centre) / 5 on the row itself, shift 4
-                    int aa = 6 * A[bi] + 5 * (A[bi - 1] + A[bi + 1]);
-                    int bb = 6 * B[bi] + 5 * (B[bi - 1] + B[bi + 1]);
-                    first[j * 2 + q] = round2i(aa * orig + bb, 8);
-                } else {      // the odd rows above and below, shift 5
-                    const int up = bi - kBox, dn = bi + kBox;
-                    int aa = 6 * (A[up] + A[dn]) + 5 * (A[up - 1] + A[up + 1] + A[dn - 1] + A[dn + 1]);
-                    int bb = 6 * (B[up] + B[dn]) + 5 * (B[up - 1] + B[up + 1] + B[dn - 1] + B[dn + 1]);
-                    first[j * 2 + q] = round2i(aa * orig + bb, 9);
-                }
-            }
+        box_pass<2>(S, A0, B0, a2tab, Vw, R, C, y_lo, true, bd, (unsigned)(((1 << 20) + n2e / 2) / n2e));
     }
     if (r1 != 0) {
         const int n2e = 9 * 9 * e1;
-        __syncthreads();  // a2tab, and pass-0 readers of A/B are done
-        box_pass<1>(S, A, B, a2tab, R, C, y_lo, false, bd, (unsigned)(((1 << 20) + n2e / 2) / n2e));
-        __syncthreads();
+        box_pass<1>(S, A1, B1, a2tab, Vw, R, C, y_lo, false, bd, (unsigned)(((1 << 20) + n2e / 2) / n2e));
     }
+    __syncthreads();
+
+    // Pixels of this thread: rows k0 .. k0+7 (k0 = 8 warp) of columns lane
+    // and lane + 32; pixel row k is box row k + 1.  Walking down its rows, a
+    // thread reads each box row of A / B once.
+    //   radius 2 (box rows of odd y only; y_lo is even, so pixel row k0 + j
+    //   has odd y when j is odd): with g = 6 A[c] + 5 (A[c-1] + A[c+1]) of a
+    //   box row, an odd row takes g of its own box row (shift 8), an even
+    //   row g of the box rows above and below (shift 9);
+    //   radius 1: 4 (A[c-1] + A[c] + A[c+1]) of the box row itself, 3 x the
+    //   same three of the rows above and below, plus A[c] of those two --
+    //   weight 4 on the cross, 3 on the corners.  Likewise for b.
     const int w0 = u.xqd[0], w1 = u.xqd[1];
+    const int k0 = 8 * warp;
+    if (k0 >= R) return;
+#pragma unroll 1
+    for (int q = 0; q < 2; ++q) {
+        const int c = lane + 32 * q;
+        if (c >= C) continue;
+        auto g0 = [&](int br, int& ga, int& gb) {  // br even: compact row br / 2
+            const int i = (br >> 1) * kBox + c + 1;
+            ga = 5 * (A0[i - 1] + A0[i + 1]) + 6 * A0[i];
+            gb = 5 * (B0[i - 1] + B0[i + 1]) + 6 * B0[i];
+        };
+        int h3a[3], h3b[3], ca[3], cb[3];
+        auto row1 = [&](int br, int slot) {
+            const int i = br * kBox + c + 1;
+            ca[slot] = A1[i];
+            cb[slot] = B1[i];
+            h3a[slot] = A1[i - 1] + ca[slot] + A1[i + 1];
+            h3b[slot] = B1[i - 1] + cb[slot] + B1[i + 1];
+        };
+        int pa = 0, pb = 0, na = 0, nb = 0;
+        if (r0) g0(k0, pa, pb);
+        if (r1) {
+            row1(k0, 0);
+            row1(k0 + 1, 1);
+        }
 #pragma unroll
-    for (int j = 0; j < kPix / 2; ++j)
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int k = warp + kWarps * j, c = lane + 32 * q;
-            if (k >= R || c >= C) continue;
+        for (int j = 0; j < 8; ++j) {
+            const int k = k0 + j;
             const int orig = S[(k + 3) * kSPitch + kSOff + c];
-            const int f0 = r0 ? first[j * 2 + q] : orig << 4;
-            int f1 = orig << 4;
+            int f0 = orig << 4, f1 = orig << 4;
+            if (r0) {
+                if ((j & 1) == 0) {
+                    g0(k + 2, na, nb);
+                    f0 = round2i((pa + na) * orig + (pb + nb), 9);
+                } else {
+                    f0 = round2i(na * orig + nb, 8);
+                    pa = na;
+                    pb = nb;
+                }
+            }
             if (r1) {
-                const int bi = (k + 1) * kBox + (c + 1), up = bi - kBox, dn = bi + kBox;
-                int aa = 4 * (A[bi] + A[bi - 1] + A[bi + 1] + A[up] + A[dn]) +
-                         3 * (A[up - 1] + A[up + 1] + A[dn - 1] + A[dn + 1]);
-                int bb = 4 * (B[bi] + B[bi - 1] + B[bi + 1] + B[up] + B[dn]) +
-                         3 * (B[up - 1] + B[up + 1] + B[dn - 1] + B[dn + 1]);
+                row1(k + 2, (j + 2) % 3);
+                const int u_ = j % 3, m_ = (j + 1) % 3, d_ = (j + 2) % 3;
+                const int aa = 4 * h3a[m_] + 3 * (h3a[u_] + h3a[d_]) + ca[u_] + ca[d_];
+                const int bb = 4 * h3b[m_] + 3 * (h3b[u_] + h3b[d_]) + cb[u_] + cb[d_];
                 f1 = round2i(aa * orig + bb, 9);
             }
-            int v = round2i(w0 * f0 + w1 * (orig << 4) + (128 - w0 - w1) * f1, 11);
-            P.out.data[(long)(y_lo + k) * P.out.stride + x_lo + c] = (uint16_t)clampi(v, 0, maxv);
+            if (k < R) {
+                const int v = round2i(w0 * f0 + w1 * (orig << 4) + (128 - w0 - w1) * f1, 11);
+                P.out.data[(long)(y_lo + k) * P.out.stride + x_lo + c] = (uint16_t)clampi(v, 0, maxv);
+            }
         }
+    }
 }
 
 
