@@ -60,17 +60,20 @@ struct PlaneMut {
 
 int ilog2_u32(uint32_t v) { return 31 - __builtin_clz(v); }
 
-// Run fn(lo, hi) over [0, n) split into `threads` contiguous ranges.
+// Run fn(lo, hi, slot) over [0, n) split into `threads` contiguous ranges
+// (slot = the range's index).  Callers flatten 2-D work (rows x column
+// blocks) in raster order, so a thin band still spreads over every thread
+// and each range's first error is its earliest in raster order.
 template <class F>
-void parallel_rows(int n, int threads, F fn) {
-    if (threads <= 1 || n < 2 * threads) {
-        fn(0, n);
+void parallel_for(long n, int threads, F fn) {
+    if (threads <= 1 || n < 2L * threads) {
+        fn(0L, n, 0);
         return;
     }
     std::vector<std::thread> pool;
     for (int t = 0; t < threads; ++t) {
-        int lo = (int)((long)n * t / threads), hi = (int)((long)n * (t + 1) / threads);
-        pool.emplace_back([=] { fn(lo, hi); });
+        long lo = n * t / threads, hi = n * (t + 1) / threads;
+        pool.emplace_back([=] { fn(lo, hi, t); });
     }
     for (auto& th : pool) th.join();
 }
@@ -222,10 +225,11 @@ int cdef_frame(const PlaneRef src[3], PlaneMut dst[3], int num_planes,
     // records its first error and the earliest one wins.
     std::vector<long> first_key(threads > 0 ? threads : 1, -1);
     std::vector<int> first_msg(first_key.size(), 0);
-    auto work = [&](int lo, int hi, int slot) {
-        for (int br = lo; br < hi; ++br) {
-            int r = br * 2;
-            for (int c = 0; c < mi_cols; c += 2) {
+    const int block_cols = (mi_cols + 1) / 2;
+    auto work = [&](long lo, long hi, int slot) {
+        for (long i = lo; i < hi; ++i) {
+            const int r = (int)(i / block_cols) * 2, c = (int)(i % block_cols) * 2;
+            {
                 long sidx = (long)(r >> 4) * cdef_stride + (c >> 4);
                 int index = (sidx >= 0 && sidx < cdef_count) ? cdef_idx[sidx] : -1;
                 auto skipped = [&](int row, int col) {
@@ -289,17 +293,7 @@ int cdef_frame(const PlaneRef src[3], PlaneMut dst[3], int num_planes,
             }
         }
     };
-    int nt = (int)first_key.size();
-    if (nt <= 1 || block_rows < 2 * nt) {
-        work(0, block_rows, 0);
-    } else {
-        std::vector<std::thread> pool;
-        for (int t = 0; t < nt; ++t) {
-            int lo = (int)((long)block_rows * t / nt), hi = (int)((long)block_rows * (t + 1) / nt);
-            pool.emplace_back([=, &work] { work(lo, hi, t); });
-        }
-        for (auto& th : pool) th.join();
-    }
+    parallel_for((long)block_rows * block_cols, (int)first_key.size(), work);
     long best = -1;
     int msg = 0;
     for (size_t t = 0; t < first_key.size(); ++t)
@@ -357,9 +351,12 @@ int upscale_plane(const PlaneRef& in, int visible_width, int output_width, int h
     const int64_t init = subpel_start(vis, outw, step);
     const int64_t max_sample = (1LL << bit_depth) - 1;
     std::vector<long> first_row(threads > 1 ? threads : 1, -1);
-    auto work = [&](int lo, int hi, int slot) {
-        for (int y = lo; y < hi; ++y)
-            for (int64_t x = 0; x < outw; ++x) {
+    const long segs = (long)((outw + 255) / 256);  // 256-sample row segments
+    auto work = [&](long lo, long hi, int slot) {
+        for (long i = lo; i < hi; ++i) {
+            const int y = (int)(i / segs);
+            const int64_t x0 = (i % segs) * 256;
+            for (int64_t x = x0; x < std::min(x0 + 256, outw); ++x) {
                 int64_t src_x = -(1 << 14) + init + x * step;
                 int64_t src_px = src_x >> 14;
                 int phase = (int)((src_x & ((1 << 14) - 1)) >> 8);
@@ -376,18 +373,9 @@ int upscale_plane(const PlaneRef& in, int visible_width, int output_width, int h
                 int64_t rounded = (sum + 64) >> 7;
                 out.set(x, y, (uint16_t)std::min(std::max(rounded, (int64_t)0), max_sample));
             }
-    };
-    int nt = (int)first_row.size();
-    if (nt <= 1 || height < 2 * nt) {
-        work(0, height, 0);
-    } else {
-        std::vector<std::thread> pool;
-        for (int t = 0; t < nt; ++t) {
-            int lo = (int)((long)height * t / nt), hi = (int)((long)height * (t + 1) / nt);
-            pool.emplace_back([=, &work] { work(lo, hi, t); });
         }
-        for (auto& th : pool) th.join();
-    }
+    };
+    parallel_for((long)height * segs, (int)first_row.size(), work);
     for (long r : first_row)
         if (r >= 0) return VACO_AV1_MSG_SR_SAMPLE;
     return 0;
@@ -559,10 +547,12 @@ int restore_plane(const PlaneRef& before, const PlaneRef& after, const LrConfig&
         for (int y = 0; y < cfg.height; ++y)
             for (int x = 0; x < cfg.width; ++x)
                 if (p->get_clamped(x, y) > max) return VACO_AV1_MSG_LR_SAMPLE;
-    parallel_rows(cfg.height, threads, [&](int lo, int hi) {
-        for (int y = lo; y < hi; ++y) {
+    const long segs = (cfg.width + 63) / 64;  // 64-sample row segments
+    parallel_for((long)cfg.height * segs, threads, [&](long lo, long hi, int) {
+        for (long i = lo; i < hi; ++i) {
+            const int y = (int)(i / segs), x0 = (int)(i % segs) * 64;
             Source src(before, after, cfg, y);
-            for (int x = 0; x < cfg.width; ++x) {
+            for (int x = x0; x < std::min(x0 + 64, cfg.width); ++x) {
                 const vaco_av1_lr_unit& u = units[cfg.unit_index(x, y, cols, rows)];
                 int64_t value;
                 if (u.type == VACO_AV1_LR_WIENER)
@@ -758,10 +748,10 @@ int deblock_frame(PlaneMut pic[3], int num_planes, const vaco_av1_frame_info& in
         int nrows = (info.mi_rows + row_step - 1) / row_step;
         for (int pass = 0; pass < 2; ++pass) {
             // Edges within one pass never overlap, so rows run independently.
-            parallel_rows(nrows, threads, [&](int lo, int hi) {
-                for (int rr = lo; rr < hi; ++rr)
-                    for (int col = 0; col < info.mi_cols; col += col_step)
-                        d.edge(pic[plane], plane, pass, rr * row_step, col);
+            const long ncols = (info.mi_cols + col_step - 1) / col_step;
+            parallel_for((long)nrows * ncols, threads, [&](long lo, long hi, int) {
+                for (long i = lo; i < hi; ++i)
+                    d.edge(pic[plane], plane, pass, (int)(i / ncols) * row_step, (int)(i % ncols) * col_step);
             });
         }
     }
