@@ -106,12 +106,31 @@ VACO_AV1_API int32_t vaco_av1_ctx_last_cuda_error(const vaco_av1_ctx* ctx);
 /* Number of kernel launches this context has issued (for launch accounting). */
 VACO_AV1_API uint64_t vaco_av1_ctx_launch_count(const vaco_av1_ctx* ctx);
 
+/* Deferred status (no counterpart in vaco, whose calls are synchronous).  By
+ * default vaco_av1_postfilter_frame_dev synchronizes its stream before it
+ * returns, to report the first error the device found in that frame, as
+ * vaco's Result does.  With deferred status enabled it enqueues the chain and
+ * returns after the host-side checks only, so a decoder can keep frames
+ * flowing with no host round trip between them.  Device-side errors then
+ * accumulate in the context: vaco_av1_ctx_flush() synchronizes `stream`,
+ * returns the earliest error (lowest stage, then raster position, then
+ * check) of every frame since the previous flush, and clears it.  Output
+ * planes of a frame are valid once the stream has passed it.  Enabling or
+ * disabling synchronizes the device.  Every other entry point stays
+ * synchronous and starts from a clear word, so flush before calling one. */
+VACO_AV1_API int32_t vaco_av1_ctx_set_deferred_status(vaco_av1_ctx* ctx, int32_t enable);
+VACO_AV1_API int32_t vaco_av1_ctx_flush(vaco_av1_ctx* ctx, void* stream, int32_t* msg);
+
 /* Per-stage device timing (no counterpart in vaco, whose profiling is
  * perf-based: crates/tool/vaco-bench/src/perf_stat.rs).  While enabled, the
  * chain and batch entry points record a CUDA event pair around each stage on
  * the stream the stage runs on; vaco_av1_ctx_stage_ms() returns the summed
- * milliseconds per stage (0 deblock, 1 CDEF, 2 superres, 3 restoration) and
- * the number of timed frames since timing was (re)enabled. */
+ * milliseconds per stage (0 deblocking + CDEF, which the chain runs as one
+ * fused kernel; 1 empty in the chain; 2 superres; 3 restoration) and the
+ * number of timed frames since timing was (re)enabled.  `enable` > 1 times
+ * one frame in `enable` (each timed frame records five events, which take
+ * stream time of their own).  Frames enqueued under deferred status are
+ * timed too; their events are read at the flush. */
 VACO_AV1_API int32_t vaco_av1_ctx_set_stage_timing(vaco_av1_ctx* ctx, int32_t enable);
 VACO_AV1_API int32_t vaco_av1_ctx_stage_ms(const vaco_av1_ctx* ctx, double* ms4, uint64_t* frames);
 

@@ -20,6 +20,8 @@ SIGNATURES = [
     ("vaco_av1_ctx_destroy", None, [_vp]),
     ("vaco_av1_ctx_last_cuda_error", _i32, [_vp]),
     ("vaco_av1_ctx_launch_count", _u64, [_vp]),
+    ("vaco_av1_ctx_set_deferred_status", _i32, [_vp, _i32]),
+    ("vaco_av1_ctx_flush", _i32, [_vp, _vp, _vp]),
     ("vaco_av1_ctx_set_stage_timing", _i32, [_vp, _i32]),
     ("vaco_av1_ctx_stage_ms", _i32, [_vp, _vp, _vp]),
     ("vaco_av1_cdef_find_direction_dev", _i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _pi32]),

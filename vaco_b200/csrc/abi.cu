@@ -313,8 +313,9 @@ void vaco_av1_ctx_destroy(vaco_av1_ctx* ctx) {
         if (b.p) cudaFree(b.p);
     if (ctx->status) cudaFree(ctx->status);
     if (ctx->status_host) cudaFreeHost(ctx->status_host);
-    for (auto& ev : ctx->marks)
-        if (ev) cudaEventDestroy(ev);
+    for (auto& frame : ctx->marks)
+        for (auto& ev : frame)
+            if (ev) cudaEventDestroy(ev);
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
     if (ctx->batch_table_host) cudaFreeHost(ctx->batch_table_host);
     if (ctx->batch_status_host) cudaFreeHost(ctx->batch_status_host);
@@ -325,15 +326,42 @@ void vaco_av1_ctx_destroy(vaco_av1_ctx* ctx) {
 int32_t vaco_av1_ctx_last_cuda_error(const vaco_av1_ctx* ctx) { return ctx ? ctx->last_cuda_error : 0; }
 uint64_t vaco_av1_ctx_launch_count(const vaco_av1_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int32_t vaco_av1_ctx_set_deferred_status(vaco_av1_ctx* ctx, int32_t enable) {
+    if (!ctx) return VACO_AV1_INVALID_DATA;
+    cudaSetDevice(ctx->device);
+    // Start from a clean word; the caller has no work of this context in flight.
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaMemset(ctx->status, 0xFF, sizeof(DeviceStatus)) != cudaSuccess)
+        return VACO_AV1_DEVICE_ERROR;
+    ctx->deferred = enable != 0;
+    return VACO_AV1_OK;
+}
+
+int32_t vaco_av1_ctx_flush(vaco_av1_ctx* ctx, void* stream, int32_t* msg) {
+    if (!ctx) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const int32_t st = finish(ctx, s, kNoError, msg);
+    if (st == VACO_AV1_DEVICE_ERROR) return st;
+    cudaError_t e = reset_status(ctx, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    return st;
+}
+
 int32_t vaco_av1_ctx_set_stage_timing(vaco_av1_ctx* ctx, int32_t enable) {
     if (!ctx) return VACO_AV1_INVALID_DATA;
     cudaSetDevice(ctx->device);
     if (enable) {
-        for (auto& ev : ctx->marks)
-            if (!ev && cudaEventCreate(&ev) != cudaSuccess) return VACO_AV1_DEVICE_ERROR;
+        for (auto& frame : ctx->marks)
+            for (auto& ev : frame)
+                if (!ev && cudaEventCreate(&ev) != cudaSuccess) return VACO_AV1_DEVICE_ERROR;
     }
-    ctx->timing = enable != 0;
-    ctx->marks_pending = false;
+    // Frames still being timed are dropped: wait for them before the reset.
+    if (ctx->mark_head != ctx->mark_tail) cudaDeviceSynchronize();
+    ctx->timing = enable > 0;
+    ctx->timing_every = enable > 0 ? enable : 1;
+    ctx->timing_count = 0;
+    ctx->mark_head = ctx->mark_tail = 0;
     for (double& v : ctx->stage_ms) v = 0;
     ctx->timed_frames = 0;
     return VACO_AV1_OK;
@@ -715,14 +743,16 @@ static bool chain_geometry_ok(const vaco_av1_frame_job* j) {
 // The chain on device pointers.  Deblocking and CDEF run fused
 // (dbcdef.cu): the deblocked picture exists only as restoration's compact
 // stripe-boundary rows.
-static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_frame_job* job, int32_t* msg) {
+static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_frame_job* job, int32_t* msg,
+                                   bool defer) {
     const vaco_av1_frame_info& info = job->info;
     const int np = info.monochrome ? 1 : 3;
     const int ssx = info.subsampling_x, ssy = info.subsampling_y;
     const bool superres = info.upscaled_width != info.coded_width;
     bool lr_active = false;
     for (int k = 0; k < np; ++k) lr_active = lr_active || job->lr_type[k] != VACO_AV1_FRAME_LR_NONE;
-    cudaError_t e = reset_status(ctx, s);
+    // With deferred status the word keeps accumulating until the next flush.
+    cudaError_t e = defer ? cudaSuccess : reset_status(ctx, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
 
     vaco_av1_picture cdef;
@@ -877,6 +907,15 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
         }
     }
     ctx->mark(4, s);
+    if (defer) {
+        // Host-side failures are known now; device-side ones wait for the flush.
+        if (hk != kNoError) {
+            set_msg(msg, (int)(hk & 0xFF));
+            return VACO_AV1_INVALID_DATA;
+        }
+        set_msg(msg, VACO_AV1_MSG_NONE);
+        return VACO_AV1_OK;
+    }
     return finish(ctx, s, hk, msg);
 }
 
@@ -884,7 +923,7 @@ int32_t vaco_av1_postfilter_frame_dev(vaco_av1_ctx* ctx, void* stream, const vac
     if (!ctx || !job) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
     if (!chain_geometry_ok(job)) return invalid(msg, VACO_AV1_MSG_FRAME_GEOMETRY);
     cudaSetDevice(ctx->device);
-    return postfilter_dev_impl(ctx, (cudaStream_t)stream, job, msg);
+    return postfilter_dev_impl(ctx, (cudaStream_t)stream, job, msg, ctx->deferred);
 }
 
 int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job, int32_t* msg) {
@@ -927,7 +966,7 @@ int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_j
         }
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
-    int32_t st = postfilter_dev_impl(ctx, s, &d, msg);
+    int32_t st = postfilter_dev_impl(ctx, s, &d, msg, false);
     if (st != VACO_AV1_OK) return st;
     e = copy_picture_out(&d.dst, &job->dst, np, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -20,28 +20,47 @@ struct vaco_av1_ctx {
     unsigned long long* status_host = nullptr;  // pinned
     int last_cuda_error = 0;
     uint64_t launches = 0;
-    // stage timing (vaco_av1_ctx_set_stage_timing)
+    // deferred status (vaco_av1_ctx_set_deferred_status): chain calls on
+    // device pointers enqueue and return; vaco_av1_ctx_flush reads the word
+    bool deferred = false;
+    // stage timing (vaco_av1_ctx_set_stage_timing): five events per frame,
+    // from a ring of kMarkRing frames so that frames enqueued under deferred
+    // status are all timed; a frame's events are read once its last one has
+    // completed.
+    static constexpr int kMarkRing = 128;
     bool timing = false;
-    bool marks_pending = false;
-    cudaEvent_t marks[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    int timing_every = 1;        // time one frame in this many
+    uint64_t timing_count = 0;   // frames seen while timing
+    bool timing_this = false;    // the current frame is timed
+    cudaEvent_t marks[kMarkRing][5] = {};
+    uint64_t mark_head = 0, mark_tail = 0;  // frames recorded / frames read
     double stage_ms[4] = {0, 0, 0, 0};
     uint64_t timed_frames = 0;
 
-    void mark(int i, cudaStream_t s) {
-        if (timing && marks[i]) {
-            cudaEventRecord(marks[i], s);
-            if (i == 4) marks_pending = true;
+    void read_marks(int slot) {
+        for (int i = 0; i < 4; ++i) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, marks[slot][i], marks[slot][i + 1]) == cudaSuccess) stage_ms[i] += ms;
         }
+        ++timed_frames;
+    }
+    void mark(int i, cudaStream_t s) {
+        if (!timing) return;
+        if (i == 0) timing_this = timing_count++ % (uint64_t)timing_every == 0;
+        if (!timing_this) return;
+        if (i == 0 && mark_head - mark_tail == kMarkRing) {
+            // the ring is full: wait for the oldest frame and read it
+            const int old = (int)(mark_tail % kMarkRing);
+            cudaEventSynchronize(marks[old][4]);
+            read_marks(old);
+            ++mark_tail;
+        }
+        cudaEventRecord(marks[mark_head % kMarkRing][i], s);
+        if (i == 4) ++mark_head;
     }
     // Called after the stream has been synchronized.
     void collect_marks() {
-        if (!marks_pending) return;
-        marks_pending = false;
-        for (int i = 0; i < 4; ++i) {
-            float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, marks[i], marks[i + 1]) == cudaSuccess) stage_ms[i] += ms;
-        }
-        ++timed_frames;
+        for (; mark_tail < mark_head; ++mark_tail) read_marks((int)(mark_tail % kMarkRing));
     }
     struct Buf {
         void* p = nullptr;
@@ -62,7 +81,12 @@ struct vaco_av1_ctx {
     void* scratch(int slot, size_t bytes) {
         Buf& b = bufs[slot];
         if (b.n >= bytes && b.p) return b.p;
-        if (b.p) cudaFree(b.p);
+        // Work enqueued without a host sync (deferred status) may still use
+        // the old buffer: let it finish before the buffer goes.
+        if (b.p) {
+            cudaDeviceSynchronize();
+            cudaFree(b.p);
+        }
         b.p = nullptr;
         b.n = 0;
         size_t n = vaco::align_up(bytes < 256 ? 256 : bytes, 256);

@@ -274,9 +274,9 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
         if (PASS == 0) {
             filter_line_class<1>(cls, smem + a.plane_off[p] + off + line * pitch, 1, nq, np, s, a.bit_depth);
         } else {
-            uint16_t* q = smem + a.plane_off[p] + off + line;
-            if (pitch == 64 + 2 * kHalo) filter_line_class<64 + 2 * kHalo>(cls, q, pitch, nq, np, s, a.bit_depth);
-            else filter_line_class<32 + 2 * kHalo>(cls, q, pitch, nq, np, s, a.bit_depth);
+            // One body for both pitches: a second copy costs more in
+            // instruction fetch than the runtime stride saves.
+            filter_line_class<0>(cls, smem + a.plane_off[p] + off + line, pitch, nq, np, s, a.bit_depth);
         }
     }
     __syncthreads();

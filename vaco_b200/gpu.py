@@ -157,6 +157,17 @@ class Context:
         st = lib().vaco_av1_postfilter_frame_dev(self.handle, stream, C.byref(dev.job), C.byref(m))
         _check(self, st, m)
 
+    def set_deferred_status(self, enable: bool) -> None:
+        """postfilter_frame_dev enqueues without a host sync; flush() reports errors."""
+        if lib().vaco_av1_ctx_set_deferred_status(self.handle, 1 if enable else 0) != abi.OK:
+            raise VacoError(abi.DEVICE_ERROR, abi.MSG["CUDA"], "could not switch deferred status")
+
+    def flush(self, stream=None) -> None:
+        """Synchronize `stream` and raise the earliest error of the frames since the last flush."""
+        m = C.c_int32()
+        st = lib().vaco_av1_ctx_flush(self.handle, stream, C.byref(m))
+        _check(self, st, m)
+
     # ------------------------------------------------------------ batched form
     @property
     def tuning(self) -> abi.Tuning:
