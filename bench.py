@@ -386,6 +386,108 @@ def run_gpu(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def run_emit(args, world, rank, local):
+    """--mode emit: pic_to_frame on the device (vaco_av1_emit_frame_dev).
+
+    A stream kernel: bytes = the u16 planes read once + the packed frame
+    written once.  Eight pictures rotate (more than L2 holds) and the step
+    count is fixed so the run stays short."""
+    import torch
+
+    from vaco_b200 import abi
+    from vaco_b200._lib import lib
+    from vaco_b200.frame import frame_layout, picture_struct
+    from vaco_b200.gpu import Context
+
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    stream = torch.cuda.current_stream(local)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    lines = []
+    for name, (w, h, bd) in {"emit_4k_10bit": (3840, 2160, 10), "emit_1080p_8bit": (1920, 1080, 8)}.items():
+        info = abi.FrameInfo()
+        info.bit_depth, info.subsampling_x, info.subsampling_y = bd, 1, 1
+        info.upscaled_width, info.coded_width, info.coded_height = w, w, h
+        info.mi_cols, info.mi_rows = 2 * ((w + 7) >> 3), 2 * ((h + 7) >> 3)
+        shapes = [(h, w), (h // 2, w // 2), (h // 2, w // 2)]
+        gen = torch.Generator(device="cuda").manual_seed(w)
+        pics, outs, args_c = [], [], []
+        for _ in range(8):
+            planes = [torch.randint(0, 1 << bd, s, dtype=torch.int16, device="cuda", generator=gen) for s in shapes]
+            frame = [torch.zeros(b.shape, dtype=torch.uint8, device="cuda") for b in frame_layout(info)]
+            fb = abi.FrameBuffer()
+            for k, t in enumerate(frame):
+                fb.planes[k] = t.data_ptr()
+                fb.linesize[k] = t.shape[1]
+            pics.append(planes)
+            outs.append(frame)
+            args_c.append((picture_struct([t.data_ptr() for t in planes], shapes), fb))
+        m = C.c_int32()
+        sptr = C.c_void_p(stream.cuda_stream)
+
+        def step(i):
+            pic, fb = args_c[i % 8]
+            if lib().vaco_av1_emit_frame_dev(ctx.handle, sptr, C.byref(pic), C.byref(info), C.byref(fb),
+                                             C.byref(m)) != abi.OK:
+                raise RuntimeError(f"emit failed: {abi.MESSAGES.get(m.value)}")
+
+        for i in range(max(args.warmup, 3)):
+            step(i)
+        steps = 400
+        # The device entry point only enqueues, so the launches run back to back.
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(steps):
+            step(i)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        bytes_in = sum(a * b for a, b in shapes) * 2
+        bytes_out = sum(a * b for a, b in shapes) * (2 if bd > 8 else 1)
+        gbs = (bytes_in + bytes_out) / (ms / 1e3) / 1e9
+        lines.append({"workload": name, "ms_per_frame": round(ms, 5), "bytes_per_frame": bytes_in + bytes_out,
+                      "achieved_gbs": round(gbs, 1), "frac_of_hbm": round(gbs / hbm_peak, 4),
+                      "mpixel_s": round(w * h / (ms / 1e3) / 1e6, 1)})
+    # End to end from host buffers (pinned): the chain alone returning u16
+    # planes, against the chain followed by emission returning the packed
+    # frame (half the bytes back at 8 bits).
+    from vaco_b200.frame import frame_buffer, pinned_copy
+
+    e2e = []
+    for wl in (synth.BATCH_MIX[1][0], synth.CONFIG1):
+        f = synth.make_frame(wl, synth.seed_for(3, 9100))
+        pf, outs, job = pinned_copy(f)
+        frame = [torch.from_numpy(b).pin_memory().numpy() for b in frame_layout(f.info())]
+        fb = frame_buffer(frame)
+        m = C.c_int32()
+        res = {"workload": wl.name}
+        ctx2 = Context(local)
+        calls = {
+            "chain_u16_out": (lambda: lib().vaco_av1_postfilter_frame_host(ctx2.handle, C.byref(job), C.byref(m)),
+                              sum(o.nbytes for o in outs)),
+            "chain_then_emit": (lambda: lib().vaco_av1_postfilter_frame_emit_host(ctx2.handle, C.byref(job),
+                                                                                  C.byref(fb), C.byref(m)),
+                                sum(b.nbytes for b in frame)),
+        }
+        for label, (call, d2h) in calls.items():
+            for _ in range(3):
+                assert call() == abi.OK
+            n = 50
+            t0 = time.perf_counter()
+            for _ in range(n):
+                assert call() == abi.OK
+            dt = (time.perf_counter() - t0) / n
+            res[label] = {"mpixel_s": round(f.output_pixels / dt / 1e6, 1), "d2h_bytes": int(d2h)}
+        ctx2.close()
+        e2e.append(res)
+    ctx.close()
+    if rank == 0:
+        print(json.dumps({"metric": "AV1 frame emission (pic_to_frame) GB/s on the device", "mode": "emit",
+                          "unit": "GB/s", "peak": hbm_peak, "lines": lines, "e2e_host": e2e}), flush=True)
+
+
 def run_batch(args, world, rank, local):
     """Config 3: 64 frames of mixed sizes (16 each of 640x360 8-bit, 1280x720
     8-bit, 1920x1080 10-bit, 3840x2160 10-bit), independently seeded, through
@@ -444,7 +546,7 @@ def main():
     ap.add_argument("--impl", default="vaco_b200", choices=["vaco_b200", "reference"])
     ap.add_argument("--workload", default="chain_4k_10bit", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--mode", default="headline", choices=["headline", "batch", "serve"])
+    ap.add_argument("--mode", default="headline", choices=["headline", "batch", "serve", "emit"])
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="seconds per arrival rate in --mode serve")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -454,6 +556,9 @@ def main():
         return
     if args.mode == "batch":
         run_batch(args, world, rank, local)
+        return
+    if args.mode == "emit":
+        run_emit(args, world, rank, local)
         return
     if args.mode == "serve":
         from vaco_b200 import serve

@@ -86,7 +86,8 @@ typedef enum vaco_av1_msg {
     VACO_AV1_MSG_SCRATCH_LIMIT = 18,      /* request exceeds a fixed scratch size */
     VACO_AV1_MSG_QUEUE_FULL = 19,         /* job admission refused */
     VACO_AV1_MSG_TIMEOUT = 20,
-    VACO_AV1_MSG_COUNT = 21
+    VACO_AV1_MSG_PIXEL_FORMAT = 21,       /* src/decode.rs:3819 */
+    VACO_AV1_MSG_COUNT = 22
 } vaco_av1_msg;
 
 /* Static, NUL-terminated text for a message id ("" for unknown ids). */
@@ -467,6 +468,41 @@ VACO_AV1_API int32_t vaco_av1_server_upload(vaco_av1_server* server, int32_t str
                                             const vaco_av1_frame_job* host);
 VACO_AV1_API int32_t vaco_av1_server_download(vaco_av1_server* server, int32_t stream_id, int32_t slot,
                                               const vaco_av1_picture* host);
+
+/* ---------------------------------------------------------------- frame emission */
+
+/* Destination planes of an emitted frame (Y, U, V; U and V unused for
+ * monochrome), in the layout vaco's Frame::alloc_video gives them
+ * (crates/model/vaco-frame/src/alloc.rs:58-90): each row `linesize` bytes. */
+typedef struct vaco_av1_frame_buffer {
+    void* planes[3];
+    int64_t linesize[3];
+} vaco_av1_frame_buffer;
+
+/* Replaces pic_to_frame / blit (src/decode.rs:3795-3891): packs `pic` into
+ * `out` as the frame's pixel format -- gray / yuv4xxp for 8 bits (one byte
+ * per sample; a sample above 255 becomes 0, as blit's u8 conversion does) or
+ * gray / yuv4xxp{10,12}le (little-endian u16).  Copies
+ * upscaled_width x coded_height luma samples and the chroma extents rounded
+ * up, each cut to its source plane's size; the rest of every row is left
+ * untouched.  8-bit 4:4:0 has no pixel format in vaco and fails with
+ * VACO_AV1_MSG_PIXEL_FORMAT.  _dev: device pointers (pic and out); no sample
+ * can fail, so it returns once the kernel is enqueued on `stream` and the
+ * frame is complete when the stream passes it.  _host: host pointers,
+ * synchronous. */
+VACO_AV1_API int32_t vaco_av1_emit_frame_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_picture* pic,
+                                             const vaco_av1_frame_info* info, const vaco_av1_frame_buffer* out,
+                                             int32_t* msg);
+VACO_AV1_API int32_t vaco_av1_emit_frame_host(vaco_av1_ctx* ctx, const vaco_av1_picture* pic,
+                                              const vaco_av1_frame_info* info, const vaco_av1_frame_buffer* out,
+                                              int32_t* msg);
+
+/* decode_frame's filter tail followed by pic_to_frame (src/decode.rs:553-559,
+ * :3795-3891), host memory in and out: the chain's u16 output stays on the
+ * device and only the packed frame (half the bytes at 8 bits) comes back.
+ * job->dst is ignored. */
+VACO_AV1_API int32_t vaco_av1_postfilter_frame_emit_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job,
+                                                         const vaco_av1_frame_buffer* out, int32_t* msg);
 
 /* The whole chain for callers that cannot call cudaMalloc.  No counterpart in
  * vaco (vaco allocates every intermediate picture through its Budget).

@@ -49,6 +49,7 @@ def lib():
         l.vo_restore_plane.argtypes = [vp, i32, i32, i32, vp, i32, i32, i32, vp, vp, i32, vp, i32, i32]
         l.vo_deblock_picture.argtypes = [vp, vp, vp, vp, vp, vp, vp, i32]
         l.vo_postfilter_frame.argtypes = [vp, i32]
+        l.vo_emit_frame.argtypes = [vp, vp, vp]
         _lib = l
     return _lib
 
@@ -162,3 +163,18 @@ def postfilter_frame(f: FrameInputs, threads: int | None = None):
     job = host_job(f, outs)
     m = lib().vo_postfilter_frame(C.byref(job), threads or default_threads())
     return outs, m
+
+
+# ---------------------------------------------------------------- frame emission
+def emit_frame(planes, info: abi.FrameInfo, frame):
+    """pic_to_frame / blit (decode.rs:3795-3891) into `frame`, a list of
+    uint8 arrays (rows x linesize) as frame_layout() makes them; returns
+    (frame, msg)."""
+    planes = [_u16(p) for p in planes]  # alive through the call
+    pic = picture_struct([ptr(p) for p in planes], [p.shape for p in planes])
+    out = abi.FrameBuffer()
+    for k, b in enumerate(frame):
+        out.planes[k] = b.ctypes.data
+        out.linesize[k] = b.shape[1]
+    m = lib().vo_emit_frame(C.byref(pic), C.byref(info), C.byref(out))
+    return frame, m

@@ -919,6 +919,41 @@ int vo_postfilter_frame(const vaco_av1_frame_job* job, int threads) {
 
 // Struct sizes as gcc lays them out from include/vaco_av1_gpu.h, for the
 // ctypes layout test.
+// pic_to_frame / blit (src/decode.rs:3795-3891): the pixel format from
+// (bit depth, monochrome, subsampling), then per plane the frame extents
+// (upscaled_width x coded_height, chroma rounded up) cut to the source
+// plane, each sample written as one byte (u8::try_from(v).unwrap_or(0): a
+// value above 255 becomes 0) or as two little-endian bytes above 8 bits.
+extern "C" int vo_emit_frame(const vaco_av1_picture* pic, const vaco_av1_frame_info* info,
+                             const vaco_av1_frame_buffer* out) {
+    const int bd = info->bit_depth;
+    const bool mono = info->monochrome != 0, sx = info->subsampling_x != 0, sy = info->subsampling_y != 0;
+    // The names of decode.rs:3802-3817; vaco-pixfmt knows all but yuv440p8le.
+    const bool known = (bd == 8 || bd == 10 || bd == 12) && !(bd == 8 && !mono && !sx && sy);
+    if (!known) return VACO_AV1_MSG_PIXEL_FORMAT;
+    const long w = info->upscaled_width, h = info->coded_height;
+    const long cw = (w + (1L << sx) - 1) >> sx, ch = (h + (1L << sy) - 1) >> sy;
+    const bool two_bytes = bd > 8;
+    for (int k = 0; k < (mono ? 1 : 3); ++k) {
+        PlaneRef src = plane_ref(*pic, k);
+        const long width = std::min<long>(k ? cw : w, src.width), height = std::min<long>(k ? ch : h, src.height);
+        uint8_t* dst = static_cast<uint8_t*>(out->planes[k]);
+        for (long y = 0; y < height; ++y) {
+            uint8_t* row = dst + y * out->linesize[k];
+            for (long x = 0; x < width; ++x) {
+                const uint16_t v = src.get_clamped((int)x, (int)y);
+                if (two_bytes) {
+                    row[2 * x] = (uint8_t)(v & 0xFF);
+                    row[2 * x + 1] = (uint8_t)(v >> 8);
+                } else {
+                    row[x] = v > 255 ? 0 : (uint8_t)v;
+                }
+            }
+        }
+    }
+    return 0;
+}
+
 extern "C" int vo_sizeof(const char* name) {
     struct Entry {
         const char* n;
@@ -934,6 +969,7 @@ extern "C" int vo_sizeof(const char* name) {
         {"vaco_av1_deblock_params", (int)sizeof(vaco_av1_deblock_params)},
         {"vaco_av1_frame_job", (int)sizeof(vaco_av1_frame_job)},
         {"vaco_av1_tuning", (int)sizeof(vaco_av1_tuning)},
+        {"vaco_av1_frame_buffer", (int)sizeof(vaco_av1_frame_buffer)},
     };
     for (const Entry& e : kSizes)
         if (std::strcmp(e.n, name) == 0) return e.s;

@@ -20,6 +20,9 @@ SIGNATURES = [
     ("vaco_av1_ctx_destroy", None, [_vp]),
     ("vaco_av1_ctx_last_cuda_error", _i32, [_vp]),
     ("vaco_av1_ctx_launch_count", _u64, [_vp]),
+    ("vaco_av1_emit_frame_dev", _i32, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    ("vaco_av1_emit_frame_host", _i32, [_vp, _vp, _vp, _vp, _vp]),
+    ("vaco_av1_postfilter_frame_emit_host", _i32, [_vp, _vp, _vp, _vp]),
     ("vaco_av1_ctx_set_deferred_status", _i32, [_vp, _i32]),
     ("vaco_av1_ctx_flush", _i32, [_vp, _vp, _vp]),
     ("vaco_av1_ctx_set_stage_timing", _i32, [_vp, _i32]),

@@ -39,6 +39,7 @@ MESSAGES = {
     18: "request exceeds the fixed scratch size",
     19: "job admission refused: queue or memory budget full",
     20: "bounded device wait timed out",
+    21: "vaco-codec-av1: unsupported pixel format",
 }
 MSG = {
     "NONE": 0, "CDEF_BIT_DEPTH": 1, "CDEF_SAMPLE": 2, "CDEF_BLOCK_PARAMS": 3,
@@ -46,6 +47,7 @@ MSG = {
     "LR_GEOMETRY": 8, "LR_UNIT_COUNT": 9, "LR_COEFFICIENT": 10, "LR_SAMPLE": 11,
     "LR_NO_UNIT_SIZE": 12, "DB_PARAMS": 13, "DB_SAMPLE": 14, "FRAME_GEOMETRY": 15,
     "NULL_ARGUMENT": 16, "CUDA": 17, "SCRATCH_LIMIT": 18, "QUEUE_FULL": 19, "TIMEOUT": 20,
+    "PIXEL_FORMAT": 21,
 }
 
 LR_NONE, LR_WIENER, LR_SGRPROJ = 0, 1, 2
@@ -159,6 +161,13 @@ class Tuning(C.Structure):
     ]
 
 
+class FrameBuffer(C.Structure):
+    _fields_ = [
+        ("planes", C.c_void_p * 3),
+        ("linesize", C.c_int64 * 3),
+    ]
+
+
 # numpy structured dtype with the vaco_av1_lr_unit layout (20 bytes)
 def lr_unit_dtype():
     import numpy as np
@@ -188,4 +197,5 @@ STRUCT_SIZES = {
     "vaco_av1_deblock_params": C.sizeof(DeblockParams),
     "vaco_av1_frame_job": C.sizeof(FrameJob),
     "vaco_av1_tuning": C.sizeof(Tuning),
+    "vaco_av1_frame_buffer": C.sizeof(FrameBuffer),
 }

@@ -5,6 +5,7 @@
 // common.cuh).  A status word key orders errors by (stage, position), so a
 // host-detected problem in a later stage never hides a device-detected one
 // in an earlier stage: host errors are folded into the same ordering.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -40,6 +41,7 @@ const char* const kMessages[VACO_AV1_MSG_COUNT] = {
     "request exceeds the fixed scratch size",
     "job admission refused: queue or memory budget full",
     "bounded device wait timed out",
+    "vaco-codec-av1: unsupported pixel format",
 };
 
 unsigned long long make_key(unsigned stage, unsigned long long position, unsigned msg) {
@@ -294,7 +296,8 @@ int32_t vaco_av1_ctx_create(int32_t device, vaco_av1_ctx** out) {
     vaco_av1_ctx* c = new (std::nothrow) vaco_av1_ctx();
     if (!c) return VACO_AV1_DEVICE_ERROR;
     c->device = device;
-    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->status, sizeof(DeviceStatus));
     if (e == cudaSuccess) e = cudaMallocHost(&c->status_host, sizeof(unsigned long long));
     if (e != cudaSuccess) {
@@ -719,7 +722,8 @@ int32_t vaco_av1_deblock_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture*
 
 // ---------------------------------------------------------------- whole chain
 
-static bool chain_geometry_ok(const vaco_av1_frame_job* j) {
+// check_dst = false: the caller supplies the destination itself (emission).
+static bool chain_geometry_ok(const vaco_av1_frame_job* j, bool check_dst = true) {
     const vaco_av1_frame_info& i = j->info;
     if (!info_ok(&i) || !padded_picture_ok(&j->src, &i)) return false;
     if (!av1_subsampling_ok(i.subsampling_x, i.subsampling_y)) return false;
@@ -733,8 +737,8 @@ static bool chain_geometry_ok(const vaco_av1_frame_job* j) {
         return false;
     for (int k = 0; k < np; ++k) {
         int sx = k ? i.subsampling_x : 0, sy = k ? i.subsampling_y : 0;
-        if (!j->dst.planes[k] || j->dst.width[k] != (i.upscaled_width >> sx) ||
-            j->dst.height[k] != (i.coded_height >> sy) || j->dst.stride[k] < j->dst.width[k])
+        if (check_dst && (!j->dst.planes[k] || j->dst.width[k] != (i.upscaled_width >> sx) ||
+                          j->dst.height[k] != (i.coded_height >> sy) || j->dst.stride[k] < j->dst.width[k]))
             return false;
     }
     return true;
@@ -926,11 +930,11 @@ int32_t vaco_av1_postfilter_frame_dev(vaco_av1_ctx* ctx, void* stream, const vac
     return postfilter_dev_impl(ctx, (cudaStream_t)stream, job, msg, ctx->deferred);
 }
 
-int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job, int32_t* msg) {
-    if (!ctx || !job) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
-    if (!chain_geometry_ok(job)) return invalid(msg, VACO_AV1_MSG_FRAME_GEOMETRY);
-    cudaSetDevice(ctx->device);
-    cudaStream_t s = ctx->stream;
+// The chain on a job whose pictures and side information are in host memory:
+// stages the inputs into context scratch, runs the chain into a device
+// picture `*d_out` (context scratch), and leaves the stream synchronized.
+static int32_t postfilter_from_host(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_frame_job* job,
+                                    vaco_av1_picture* d_out, int32_t* msg) {
     const vaco_av1_frame_info& info = job->info;
     const int np = info.monochrome ? 1 : 3;
     const int ssx = info.subsampling_x, ssy = info.subsampling_y;
@@ -967,11 +971,135 @@ int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_j
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
     int32_t st = postfilter_dev_impl(ctx, s, &d, msg, false);
+    *d_out = d.dst;
+    return st;
+}
+
+int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job, int32_t* msg) {
+    if (!ctx || !job) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    if (!chain_geometry_ok(job)) return invalid(msg, VACO_AV1_MSG_FRAME_GEOMETRY);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    vaco_av1_picture dst;
+    const int32_t st = postfilter_from_host(ctx, s, job, &dst, msg);
     if (st != VACO_AV1_OK) return st;
-    e = copy_picture_out(&d.dst, &job->dst, np, s);
+    cudaError_t e = copy_picture_out(&dst, &job->dst, job->info.monochrome ? 1 : 3, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
     return VACO_AV1_OK;
+}
+// ---------------------------------------------------------------- frame emission
+
+// The pixel formats pic_to_frame can name (src/decode.rs:3802-3819): every
+// AV1 layout except 8-bit 4:4:0, for which vaco-pixfmt has no "yuv440p8le".
+static bool emit_format_ok(const vaco_av1_frame_info& i) {
+    if (i.bit_depth != 8 && i.bit_depth != 10 && i.bit_depth != 12) return false;
+    if (i.subsampling_x < 0 || i.subsampling_x > 1 || i.subsampling_y < 0 || i.subsampling_y > 1) return false;
+    return !(i.bit_depth == 8 && !i.monochrome && i.subsampling_x == 0 && i.subsampling_y == 1);
+}
+
+// Per plane: pic_to_frame's extents (upscaled_width x coded_height, chroma
+// rounded up, src/decode.rs:3820-3828) cut to the source plane, as blit's
+// w.min(pic.width()) does.  Returns 0 or a message id.
+static int emit_plan(const vaco_av1_picture* pic, const vaco_av1_frame_info& i, const vaco_av1_frame_buffer* out,
+                     EmitPlane* ep, int* np_out) {
+    if (!emit_format_ok(i)) return VACO_AV1_MSG_PIXEL_FORMAT;
+    if (i.upscaled_width <= 0 || i.coded_height <= 0) return VACO_AV1_MSG_FRAME_GEOMETRY;
+    const int np = i.monochrome ? 1 : 3;
+    const int bps = i.bit_depth > 8 ? 2 : 1;
+    for (int k = 0; k < np; ++k) {
+        const int sx = k ? i.subsampling_x : 0, sy = k ? i.subsampling_y : 0;
+        const int fw = (i.upscaled_width + (1 << sx) - 1) >> sx, fh = (i.coded_height + (1 << sy) - 1) >> sy;
+        if (!pic->planes[k] || !out->planes[k]) return VACO_AV1_MSG_NULL_ARGUMENT;
+        if (pic->width[k] < 0 || pic->height[k] < 0 || pic->stride[k] < pic->width[k]) return VACO_AV1_MSG_FRAME_GEOMETRY;
+        const int w = std::min(fw, pic->width[k]), h = std::min(fh, pic->height[k]);
+        if (out->linesize[k] < (int64_t)w * bps) return VACO_AV1_MSG_FRAME_GEOMETRY;
+        ep[k] = EmitPlane{pic->planes[k], pic->stride[k], (uint8_t*)out->planes[k], out->linesize[k], w, h};
+    }
+    *np_out = np;
+    return 0;
+}
+
+int32_t vaco_av1_emit_frame_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_picture* pic,
+                                const vaco_av1_frame_info* info, const vaco_av1_frame_buffer* out, int32_t* msg) {
+    if (!ctx || !pic || !info || !out) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    EmitPlane ep[3];
+    int np = 0;
+    if (int m = emit_plan(pic, *info, out, ep, &np)) return invalid(msg, m);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    // No sample can fail emission, so nothing on the device needs reporting:
+    // the call returns once the kernel is enqueued.
+    cudaError_t e = launch_emit(ep, np, info->bit_depth > 8, ctx->sm_count, s);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    set_msg(msg, VACO_AV1_MSG_NONE);
+    return VACO_AV1_OK;
+}
+
+// Packs the device picture `dev` into context scratch and copies the packed
+// rows to the host frame `out` (one 2-D copy per plane), synchronously.
+static int32_t emit_to_host(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_picture* dev,
+                            const vaco_av1_frame_info& info, const vaco_av1_frame_buffer* out, int32_t* msg) {
+    EmitPlane ep[3];
+    int np = 0;
+    if (int m = emit_plan(dev, info, out, ep, &np)) return invalid(msg, m);
+    const int bps = info.bit_depth > 8 ? 2 : 1;
+    for (int k = 0; k < np; ++k) {
+        const long long row = (long long)align_up((size_t)std::max(ep[k].width * bps, 1), 64);
+        void* d = ctx->scratch(S_EMIT0 + k, (size_t)row * std::max(ep[k].height, 1));
+        if (!d) return cuda_fail(ctx, cudaErrorMemoryAllocation, msg);
+        ep[k].dst = (uint8_t*)d;
+        ep[k].dst_stride = row;
+    }
+    cudaError_t e = launch_emit(ep, np, bps == 2, ctx->sm_count, s);
+    ctx->launches++;
+    for (int k = 0; k < np && e == cudaSuccess; ++k)
+        if (ep[k].width > 0 && ep[k].height > 0)
+            e = cudaMemcpy2DAsync(out->planes[k], (size_t)out->linesize[k], ep[k].dst, (size_t)ep[k].dst_stride,
+                                  (size_t)ep[k].width * bps, (size_t)ep[k].height, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    set_msg(msg, VACO_AV1_MSG_NONE);
+    return VACO_AV1_OK;
+}
+
+int32_t vaco_av1_emit_frame_host(vaco_av1_ctx* ctx, const vaco_av1_picture* pic, const vaco_av1_frame_info* info,
+                                 const vaco_av1_frame_buffer* out, int32_t* msg) {
+    if (!ctx || !pic || !info || !out) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    if (!emit_format_ok(*info)) return invalid(msg, VACO_AV1_MSG_PIXEL_FORMAT);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const int np = info->monochrome ? 1 : 3;
+    for (int k = 0; k < np; ++k)
+        if (!pic->planes[k]) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    vaco_av1_picture dev;
+    cudaError_t e = cudaSuccess;
+    if (!stage_picture_in(ctx, pic, np, S_H_IN0, &dev, s, &e)) return cuda_fail(ctx, e, msg);
+    return emit_to_host(ctx, s, &dev, *info, out, msg);
+}
+
+int32_t vaco_av1_postfilter_frame_emit_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job,
+                                            const vaco_av1_frame_buffer* out, int32_t* msg) {
+    if (!ctx || !job || !out) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    if (!chain_geometry_ok(job, false)) return invalid(msg, VACO_AV1_MSG_FRAME_GEOMETRY);
+    if (!emit_format_ok(job->info)) return invalid(msg, VACO_AV1_MSG_PIXEL_FORMAT);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    // The chain's own output stays on the device, in scratch of the chain's
+    // output extents.
+    vaco_av1_frame_job j = *job;
+    const vaco_av1_frame_info& i = job->info;
+    for (int k = 0; k < 3; ++k) {
+        const int sx = k ? i.subsampling_x : 0, sy = k ? i.subsampling_y : 0;
+        j.dst.width[k] = i.upscaled_width >> sx;
+        j.dst.height[k] = i.coded_height >> sy;
+        j.dst.stride[k] = j.dst.width[k];
+    }
+    vaco_av1_picture dst;
+    const int32_t st = postfilter_from_host(ctx, s, &j, &dst, msg);
+    if (st != VACO_AV1_OK) return st;
+    return emit_to_host(ctx, s, &dst, i, out, msg);
 }
 
 }  // extern "C"

@@ -107,6 +107,7 @@ enum Slot {
     S_H_OUT0, S_H_OUT1, S_H_OUT2,     // host-entry staging (outputs)
     S_H_SIDE0, S_H_SIDE1, S_H_SIDE2, S_H_SIDE3, S_H_SIDE4, S_H_SIDE5,
     S_BATCH_ARENA, S_BATCH_TABLE,      // batched form: intermediates, per-batch tables
+    S_EMIT0, S_EMIT1, S_EMIT2,         // host-entry emission: packed frame planes
 };
 
 

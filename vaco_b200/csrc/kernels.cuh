@@ -34,6 +34,19 @@ struct SuperresPlane {
 cudaError_t launch_superres(const SuperresPlane* planes, int count, int bit_depth, DeviceStatus* status,
                             unsigned stage, cudaStream_t stream);
 
+// ---------------------------------------------------------------- frame emission
+// One plane of pic_to_frame / blit (src/decode.rs:3795-3891): `width` x
+// `height` samples of `src` (stride in samples) packed into `dst` (stride in
+// bytes), one byte per sample or, with two_bytes, a little-endian u16.
+struct EmitPlane {
+    const uint16_t* src;
+    int src_stride;
+    uint8_t* dst;
+    long long dst_stride;
+    int width, height;
+};
+cudaError_t launch_emit(const EmitPlane* planes, int count, int two_bytes, int sm_count, cudaStream_t stream);
+
 // ---------------------------------------------------------------- restoration
 struct LrPlane {
     DevPlaneC before;

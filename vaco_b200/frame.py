@@ -222,3 +222,29 @@ def pinned_copy(f: FrameInputs):
     pf.lr_units = [pin(u.view(np.uint8)).view(u.dtype) for u in f.lr_units]
     outs = [pin(o) for o in alloc_outputs(pf)]
     return pf, outs, host_job(pf, outs)
+
+
+def frame_layout(info: "abi.FrameInfo", fill: int = 0) -> List[np.ndarray]:
+    """Host planes of an emitted frame in vaco's layout (vaco-pixfmt
+    plane_layout with vaco-pool's 64-byte row alignment): rows of
+    ceil(samples * bytes per sample / 64) * 64 bytes, chroma extents rounded
+    up.  `fill` marks the bytes the emission must leave alone."""
+    bps = 2 if info.bit_depth > 8 else 1
+    out = []
+    for k in range(1 if info.monochrome else 3):
+        sx = info.subsampling_x if k else 0
+        sy = info.subsampling_y if k else 0
+        w = (info.upscaled_width + (1 << sx) - 1) >> sx
+        h = (info.coded_height + (1 << sy) - 1) >> sy
+        line = (w * bps + 63) // 64 * 64
+        out.append(np.full((h, line), fill, np.uint8))
+    return out
+
+
+def frame_buffer(planes: Sequence[np.ndarray]) -> "abi.FrameBuffer":
+    """A vaco_av1_frame_buffer over host uint8 planes (rows x linesize)."""
+    fb = abi.FrameBuffer()
+    for k, b in enumerate(planes):
+        fb.planes[k] = b.ctypes.data
+        fb.linesize[k] = b.shape[1]
+    return fb

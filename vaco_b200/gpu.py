@@ -13,7 +13,8 @@ import numpy as np
 
 from . import abi
 from ._lib import lib
-from .frame import FrameInputs, alloc_outputs, build_job, host_job, picture_struct, ptr
+from .frame import (FrameInputs, alloc_outputs, build_job, frame_buffer, frame_layout, host_job, picture_struct,
+                    ptr)
 
 
 class VacoError(Exception):
@@ -141,6 +142,29 @@ class Context:
                                                  ptr(txc), ptr(lvl), C.byref(params), C.byref(m))
         _check(self, st, m)
         return outs
+
+    def emit_frame(self, planes: Sequence[np.ndarray], info: abi.FrameInfo, fill: int = 0) -> List[np.ndarray]:
+        """pic_to_frame through the host entry point: u16 planes -> packed
+        frame planes (uint8 rows x linesize, vaco's layout)."""
+        frame = frame_layout(info, fill)
+        planes = [np.ascontiguousarray(p, np.uint16) for p in planes]  # alive through the call
+        pic = picture_struct([ptr(p) for p in planes], [p.shape for p in planes])
+        m = C.c_int32()
+        st = lib().vaco_av1_emit_frame_host(self.handle, C.byref(pic), C.byref(info), C.byref(frame_buffer(frame)),
+                                            C.byref(m))
+        _check(self, st, m)
+        return frame
+
+    def postfilter_frame_emit(self, f: FrameInputs, fill: int = 0) -> List[np.ndarray]:
+        """The chain then pic_to_frame, host arrays in, packed frame out."""
+        info = f.info()
+        frame = frame_layout(info, fill)
+        job = host_job(f, [np.zeros((1, 1), np.uint16)] * f.num_planes)
+        m = C.c_int32()
+        st = lib().vaco_av1_postfilter_frame_emit_host(self.handle, C.byref(job), C.byref(frame_buffer(frame)),
+                                                       C.byref(m))
+        _check(self, st, m)
+        return frame
 
     def postfilter_frame(self, f: FrameInputs) -> List[np.ndarray]:
         """deblock -> CDEF -> superres -> restoration through the host entry point."""
