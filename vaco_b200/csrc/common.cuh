@@ -55,15 +55,27 @@ __device__ __forceinline__ int get_clamped(const DevPlaneC& p, int x, int y) {
 __device__ __forceinline__ int round2(int v, int shift) { return shift == 0 ? v : (v + (1 << (shift - 1))) >> shift; }
 
 // AV1 TX_SIZE enum -> log2 width / height
-__host__ __device__ constexpr int tx_w_log2(int t) {
-    return t == 0 ? 2 : t == 1 ? 3 : t == 2 ? 4 : t == 3 ? 5 : t == 4 ? 6 : t == 5 ? 2 : t == 6 ? 3
-         : t == 7 ? 3 : t == 8 ? 4 : t == 9 ? 4 : t == 10 ? 5 : t == 11 ? 5 : t == 12 ? 6 : t == 13 ? 2
-         : t == 14 ? 4 : t == 15 ? 3 : t == 16 ? 5 : t == 17 ? 4 : 6;
+// log2 of Tx_Width / Tx_Height per TX_SIZE (AV1 §6.10.19 ordering), packed
+// 3 bits per size (log2 - 2) into one 64-bit immediate, so a lookup with a
+// per-lane size is a shift and a mask.  Sizes past the table (invalid input,
+// which the callers report) read as the last entry.
+struct TxLog2Table {
+    int w[19], h[19];
+};
+constexpr TxLog2Table kTxLog2 = {{2, 3, 4, 5, 6, 2, 3, 3, 4, 4, 5, 5, 6, 2, 4, 3, 5, 4, 6},
+                                 {2, 3, 4, 5, 6, 3, 2, 4, 3, 5, 4, 6, 5, 4, 2, 5, 3, 6, 4}};
+__host__ __device__ constexpr unsigned long long tx_log2_packed(bool height) {
+    unsigned long long m = 0;
+    for (int t = 0; t < 19; ++t) m |= (unsigned long long)((height ? kTxLog2.h[t] : kTxLog2.w[t]) - 2) << (3 * t);
+    return m;
 }
-__host__ __device__ constexpr int tx_h_log2(int t) {
-    return t == 0 ? 2 : t == 1 ? 3 : t == 2 ? 4 : t == 3 ? 5 : t == 4 ? 6 : t == 5 ? 3 : t == 6 ? 2
-         : t == 7 ? 4 : t == 8 ? 3 : t == 9 ? 5 : t == 10 ? 4 : t == 11 ? 6 : t == 12 ? 5 : t == 13 ? 4
-         : t == 14 ? 2 : t == 15 ? 5 : t == 16 ? 3 : t == 17 ? 6 : 4;
+__host__ __device__ inline int tx_w_log2(int t) {
+    constexpr unsigned long long m = tx_log2_packed(false);
+    return (int)((m >> (3 * (t < 18 ? t : 18))) & 7u) + 2;
+}
+__host__ __device__ inline int tx_h_log2(int t) {
+    constexpr unsigned long long m = tx_log2_packed(true);
+    return (int)((m >> (3 * (t < 18 ? t : 18))) & 7u) + 2;
 }
 
 inline int div_up(int a, int b) { return (a + b - 1) / b; }

@@ -58,6 +58,23 @@ struct SideWindow {
     uint32_t lvl[kWinCells];   // loop-filter levels (Yv, Yh, U, V) when a level map is given
 };
 
+// n / d for the few divisors the tile loops meet (segment counts per edge
+// row 9, 10, 17, 18; 16-byte vectors per staged row 6, 10; sentinel window
+// widths 36, 68).  A switch over constants lets the compiler use a multiply
+// for each instead of a general integer division.
+__device__ __forceinline__ int div_small(int n, int d) {
+    switch (d) {
+        case 6: return n / 6;
+        case 9: return n / 9;
+        case 10: return n / 10;
+        case 17: return n / 17;
+        case 18: return n / 18;
+        case 36: return n / 36;
+        case 68: return n / 68;
+        default: return n / d;
+    }
+}
+
 struct PlaneGeom {
     int tw, th;        // tile extent in this plane
     int pitch, rows;   // staged region
@@ -207,7 +224,7 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
         if (p != 0 && a.levels[1 + p] == 0) continue;
         const PlaneGeom g = p ? gc : gl;
         const int na = p ? nac : na0, nb = p ? nbc : nb0;
-        const int ia = j / nb, ib = j - ia * nb;
+        const int ia = div_small(j, nb), ib = j - ia * nb;
         const DevPlane& P = a.dst[p];
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
         const int yp = PASS == 0 ? py0 - (p ? 4 : 8) + 4 * ia : py0 + 4 * ia;
@@ -217,7 +234,7 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
                                row * 4 < a.coded_height && (PASS == 0 ? xp > 0 : yp > 0);
         if (!on_screen) continue;
         const uint8_t* map = side.tx[p ? 1 : 0];
-        const int w = ((yp - py0) / 4 + kWinTop) * kWinCols + (xp - px0) / 4 + kWinLeft;
+        const int w = (((yp - py0) >> 2) + kWinTop) * kWinCols + ((xp - px0) >> 2) + kWinLeft;  // multiples of 4
         const int cur = map[w];
         const int prev = PASS == 0 ? map[w - 1] : map[w - kWinCols];
         const int cl = PASS == 0 ? tx_w_log2(cur) : tx_h_log2(cur);
@@ -325,7 +342,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
         const int vpr = g.pitch / 8;
         for (int v = tid; v < g.rows * vpr; v += kThreads) {
-            const int r = v / vpr, cv = v - r * vpr;
+            const int r = div_small(v, vpr), cv = v - r * vpr;
             const int y = clampi(py0 - kHalo + r, 0, P.height - 1);
             const int x = px0 - kHalo + cv * 8;
             const uint16_t* row = P.data + (long)y * P.stride;
@@ -380,7 +397,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
             const int ccols = (a.mi_cols + a.ssx) >> a.ssx, crows = (a.mi_rows + a.ssy) >> a.ssy;
             const int cw = 16 >> a.ssx, ch = 16 >> a.ssy;
             for (int i = tid; i < cw * ch; i += kThreads) {
-                const int dr = i / cw, dc = i - dr * cw;
+                const int dr = i >> (4 - a.ssx), dc = i - dr * cw;  // cw = 16 >> ssx
                 const int r = (mi_r0 >> a.ssy) + dr, c = (mi_c0 >> a.ssx) + dc;
                 if (r < crows && c < ccols) bad |= s_side.tx[1][(dr + kWinTop) * kWinCols + dc + kWinLeft] > 18;
             }
@@ -397,7 +414,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
             const int cpr = g.tw / 8, rows = min(g.th, P.height - py0);
             const uint16_t* t = smem + a.plane_off[p];
             for (int v = tid; v < rows * cpr; v += kThreads) {
-                const int r = v / cpr, cv = v - r * cpr;
+                const int r = v >> (3 - g.sx), cv = v - r * cpr;  // cpr = tw / 8 = 8 >> sx
                 const int x = px0 + cv * 8;
                 if (x >= P.width) continue;
                 const uint16_t* q = t + (r + kHalo) * g.pitch + kHalo + cv * 8;
@@ -431,9 +448,10 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         const int width = a.dst[p].width, height = a.dst[p].height;
         // the tile (th rows, th a multiple of the stripe height or half of it)
         // holds boundary rows y = k*sh - off - 2 + sub, sub < 4
-        for (int i = warp; i < 4 * (g.th / sh + 1); i += kThreads / 32) {
+        const int lsh = 6 - g.sy;  // log2 of the stripe height
+        for (int i = warp; i < 4 * ((g.th >> lsh) + 1); i += kThreads / 32) {
             const int kk = i >> 2, sub = i & 3;
-            const int kb = (py0 + off + 2) / sh + kk;
+            const int kb = ((py0 + off + 2) >> lsh) + kk;
             const int y = kb * sh - off - 2 + sub;
             if (kb < 1 || y < py0 || y >= py0 + g.th || y >= height) continue;
             for (int c = lane; c < g.tw; c += 32)
@@ -468,7 +486,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         uint16_t* t = smem + a.plane_off[p];
         const int wr = g.th + 4, wc = g.tw + 4;
         for (int i = tid; i < wr * wc; i += kThreads) {
-            const int r = i / wc, c = i - r * wc;
+            const int r = div_small(i, wc), c = i - r * wc;
             const int y = py0 - 2 + r, x = px0 - 2 + c;
             if (y < 0 || x < 0 || y >= d.height || x >= d.width)
                 t[(r + kHalo - 2) * g.pitch + (c + kHalo - 2)] = (uint16_t)kSent;
