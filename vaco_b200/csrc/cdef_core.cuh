@@ -253,6 +253,15 @@ __device__ __forceinline__ uint32_t load_pair(const PairTap& t, int word_off) {
     return __byte_perm(t.w[word_off], t.w[word_off + 1], t.sel);
 }
 
+// A tap whose pair is one aligned word: of the plane itself when the pair
+// starts on an even sample, of a copy shifted by one sample when it starts
+// on an odd one.
+struct WordTap {
+    const uint32_t* w;
+};
+
+__device__ __forceinline__ uint32_t load_pair(const WordTap& t, int word_off) { return t.w[word_off]; }
+
 template <bool MASK_MAX>
 __device__ __forceinline__ void pair_tap_step(uint32_t v, uint32_t cur, uint32_t t2, int s, uint32_t smask, uint32_t w,
                                               uint32_t& accp, uint32_t& accn, uint32_t& mn, uint32_t& mx) {
@@ -282,8 +291,8 @@ __device__ __forceinline__ void pair_tap_step(uint32_t v, uint32_t cur, uint32_t
 // are the 12 tap positions of the block for this lane, `row` the word offset
 // of the current row relative to the block's first row.  MASK_MAX: the tile
 // touches a plane edge, so sentinel samples must not raise the maximum.
-template <bool MASK_MAX>
-__device__ __forceinline__ uint32_t filter_pair(uint32_t cur, const PairTap* taps, int row, const PairBlock& f,
+template <bool MASK_MAX, class Tap>
+__device__ __forceinline__ uint32_t filter_pair(uint32_t cur, const Tap* taps, int row, const PairBlock& f,
                                                 bool pri_on, bool sec_on) {
     const uint32_t tp = f.pri | ((uint32_t)f.pri << 16), ts = f.sec | ((uint32_t)f.sec << 16);
     const uint32_t pm = (0xFFFFu >> f.pri_shift) * 0x10001u, sm = (0xFFFFu >> f.sec_shift) * 0x10001u;

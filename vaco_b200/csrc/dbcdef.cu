@@ -45,6 +45,8 @@ constexpr int kHalo = 8;
 // 3 x 340), 1 = chroma size 8 (2 x 340), 2 = luma size 8, 3 = luma size 16.
 __constant__ int c_list_off[4] = {0, 1020, 1700, 2040};
 constexpr int kListTotal = 2380;
+// Rows of the luma CDEF window (th + 4) kept as odd-aligned pairs.
+constexpr int kShiftRows = 64 + 4;
 
 // Side-information window of a tile: cells [mi_r0 - kWinTop, +kWinRows) x
 // [mi_c0 - kWinLeft, +kWinCols) of the luma maps, and the same shape around
@@ -122,10 +124,13 @@ struct DbCdefArgs {
 // rows l / ppr + RPI*j.  PITCH is the staged pitch, BH the block height.
 // pri_on / sec_on: the tile preset's primary / secondary strength is
 // non-zero; with neither, every sample stays as it is.
-template <int PITCH, int BH, int RPI, bool EDGE>
-__device__ __forceinline__ void filter_pairs(const uint16_t* t, const DevPlane& d, int px0, int py0, int tw,
-                                             const uint8_t* active, const PairBlock* blocks, bool pri_on, bool sec_on,
-                                             int warp, int lane, int sx) {
+// SHIFT (luma): s1 holds the tile's luma pairs that start on odd samples,
+// kShiftRows rows from row kHalo - 2 on the staged pitch, so every tap is a
+// single aligned word.
+template <int PITCH, int BH, int RPI, bool EDGE, bool SHIFT>
+__device__ __forceinline__ void filter_pairs(const uint16_t* t, const uint32_t* s1, const DevPlane& d, int px0,
+                                             int py0, int tw, const uint8_t* active, const PairBlock* blocks,
+                                             bool pri_on, bool sec_on, int warp, int lane, int sx) {
     const int ppr = 32 / RPI;              // pairs per row
     const int lp = lane % ppr, lr = lane / ppr;
     const int x = 2 * lp;
@@ -144,17 +149,36 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const DevPlane& 
     const uint32_t* cw = reinterpret_cast<const uint32_t*>(t + base_i);
     if ((pri_on || sec_on) && active[b]) {
         const PairBlock f = blocks[b];
-        PairTap taps[12];
+        if (SHIFT) {
+            const uint32_t* t32 = reinterpret_cast<const uint32_t*>(t);
+            auto word_tap = [&](int i) {  // i: staged index of the pair's first sample
+                return WordTap{(i & 1) ? s1 + ((i >> 1) - (kHalo - 2) * (PITCH / 2)) : t32 + (i >> 1)};
+            };
+            WordTap taps[12];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            taps[2 * k] = pair_tap(t, base_i + f.off[k]);
-            taps[2 * k + 1] = pair_tap(t, base_i - f.off[k]);
-        }
+            for (int k = 0; k < 6; ++k) {
+                taps[2 * k] = word_tap(base_i + f.off[k]);
+                taps[2 * k + 1] = word_tap(base_i - f.off[k]);
+            }
 #pragma unroll 2
-        for (int j = 0; j < BH / RPI; ++j) {
-            const int woff = j * RPI * PITCH / 2;
-            const uint32_t v = filter_pair<EDGE>(cw[woff], taps, woff, f, pri_on, sec_on);
-            if (col_in && lr + RPI * j < rows_here) o[j * ostride] = v;
+            for (int j = 0; j < BH / RPI; ++j) {
+                const int woff = j * RPI * PITCH / 2;
+                const uint32_t v = filter_pair<EDGE>(cw[woff], taps, woff, f, pri_on, sec_on);
+                if (col_in && lr + RPI * j < rows_here) o[j * ostride] = v;
+            }
+        } else {
+            PairTap taps[12];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                taps[2 * k] = pair_tap(t, base_i + f.off[k]);
+                taps[2 * k + 1] = pair_tap(t, base_i - f.off[k]);
+            }
+#pragma unroll 2
+            for (int j = 0; j < BH / RPI; ++j) {
+                const int woff = j * RPI * PITCH / 2;
+                const uint32_t v = filter_pair<EDGE>(cw[woff], taps, woff, f, pri_on, sec_on);
+                if (col_in && lr + RPI * j < rows_here) o[j * ostride] = v;
+            }
         }
     } else if (col_in) {
 #pragma unroll
@@ -163,12 +187,17 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const DevPlane& 
     }
 }
 
-template <int PITCH, int BH, int RPI>
-__device__ __forceinline__ void filter_pairs_edge(bool edge, const uint16_t* t, const DevPlane& d, int px0, int py0,
-                                                  int tw, const uint8_t* active, const PairBlock* blocks, bool pri_on,
-                                                  bool sec_on, int warp, int lane, int sx) {
-    if (edge) filter_pairs<PITCH, BH, RPI, true>(t, d, px0, py0, tw, active, blocks, pri_on, sec_on, warp, lane, sx);
-    else filter_pairs<PITCH, BH, RPI, false>(t, d, px0, py0, tw, active, blocks, pri_on, sec_on, warp, lane, sx);
+template <int PITCH, int BH, int RPI, bool SHIFT>
+__device__ __forceinline__ void filter_pairs_edge(bool edge, const uint16_t* t, const uint32_t* s1, const DevPlane& d,
+                                                  int px0, int py0, int tw, const uint8_t* active,
+                                                  const PairBlock* blocks, bool pri_on, bool sec_on, int warp,
+                                                  int lane, int sx) {
+    if (edge)
+        filter_pairs<PITCH, BH, RPI, true, SHIFT>(t, s1, d, px0, py0, tw, active, blocks, pri_on, sec_on, warp, lane,
+                                                 sx);
+    else
+        filter_pairs<PITCH, BH, RPI, false, SHIFT>(t, s1, d, px0, py0, tw, active, blocks, pri_on, sec_on, warp, lane,
+                                                  sx);
 }
 
 // Segment-list entry: level (6 bits) | samples on the q side, capped at 8 (4)
@@ -307,9 +336,18 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     __shared__ int s_cost[64][8];
     __shared__ PairBlock s_pair[3][64];
     __shared__ uint8_t s_active[64];
-    __shared__ uint32_t s_list[kListTotal];  // per size class, see seg_entry()
     __shared__ int s_count[4];
-    __shared__ SideWindow s_side;
+    // The deblocking lists and side window are dead once deblocking is done;
+    // the CDEF phase reuses their space for the odd-aligned luma pairs.
+    __shared__ union {
+        struct {
+            uint32_t list[kListTotal];  // per size class, see seg_entry()
+            SideWindow side;
+        } db;
+        uint32_t shifted[kShiftRows * (64 + 2 * kHalo) / 2];
+    } s_u;
+    uint32_t* s_list = s_u.db.list;
+    SideWindow& s_side = s_u.db.side;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int mi_r0 = tile_y * 16, mi_c0 = tile_x * 16;
@@ -494,6 +532,20 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     }
     __syncthreads();
 
+    // The luma CDEF window's pairs that start on odd samples (rows kHalo-2 ..
+    // kHalo+th+1, first samples on columns kHalo-1 .. kHalo+tw-1), as words
+    // on the staged row pitch, so the pair filter reads every luma tap with
+    // one aligned load.
+    {
+        constexpr int WP = (64 + 2 * kHalo) / 2, W0 = (kHalo - 1) / 2, NW = 64 / 2 + 1;
+        const uint32_t* t32 = reinterpret_cast<const uint32_t*>(smem + a.plane_off[0]);
+        for (int i = tid; i < kShiftRows * NW; i += kThreads) {
+            const int r = i / NW, w = W0 + (i - r * NW);
+            const int src = (kHalo - 2 + r) * WP + w;
+            s_u.shifted[r * WP + w] = __byte_perm(t32[src], t32[src + 1], 0x5432);
+        }
+    }
+
     // Direction search: warp w handles direction pair (w & 3) for blocks
     // (w >> 2)*32 + lane (warp-uniform branches).
     const int lpitch = 64 + 2 * kHalo;
@@ -552,15 +604,18 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
             sec_on = (p ? a.uv_sec[index] : a.y_sec[index]) != 0;
         }
         // tile layouts: 64x64 (luma, 4:4:4 chroma), 32x32 (4:2:0), 32x64 (4:2:2)
-        if (g.tw == 64) {
-            filter_pairs_edge<64 + 2 * kHalo, 8, 1>(edge, tp, d, px0, py0, g.tw, s_active, s_pair[p], pri_on, sec_on,
-                                                    warp, lane, g.sx);
+        if (p == 0) {
+            filter_pairs_edge<64 + 2 * kHalo, 8, 1, true>(edge, tp, s_u.shifted, d, px0, py0, g.tw, s_active,
+                                                          s_pair[p], pri_on, sec_on, warp, lane, g.sx);
+        } else if (g.tw == 64) {
+            filter_pairs_edge<64 + 2 * kHalo, 8, 1, false>(edge, tp, nullptr, d, px0, py0, g.tw, s_active, s_pair[p],
+                                                           pri_on, sec_on, warp, lane, g.sx);
         } else if (g.th == 32) {
-            filter_pairs_edge<32 + 2 * kHalo, 4, 2>(edge, tp, d, px0, py0, g.tw, s_active, s_pair[p], pri_on, sec_on,
-                                                    warp, lane, g.sx);
+            filter_pairs_edge<32 + 2 * kHalo, 4, 2, false>(edge, tp, nullptr, d, px0, py0, g.tw, s_active, s_pair[p],
+                                                           pri_on, sec_on, warp, lane, g.sx);
         } else {
-            filter_pairs_edge<32 + 2 * kHalo, 8, 2>(edge, tp, d, px0, py0, g.tw, s_active, s_pair[p], pri_on, sec_on,
-                                                    warp, lane, g.sx);
+            filter_pairs_edge<32 + 2 * kHalo, 8, 2, false>(edge, tp, nullptr, d, px0, py0, g.tw, s_active, s_pair[p],
+                                                           pri_on, sec_on, warp, lane, g.sx);
         }
     }
 }
