@@ -104,16 +104,41 @@ __device__ __forceinline__ bool unit_ok(const vaco_av1_lr_unit& u) {
 // squares) of every column the row's boxes reach, in the warp's own buffer
 // V, then each box sum as 2 RAD + 1 of those -- 2 (2 RAD + 1) loads per box
 // instead of (2 RAD + 1)^2.
+// box_ab's a2 and b (restoration.rs:314-339) from a box sum and sum of
+// squares, stored at box position (ar, bc).
+template <int RAD>
+__device__ __forceinline__ void box_ab(int sum, int sum_sq, int ar, int bc, uint16_t* __restrict__ A,
+                                       int32_t* __restrict__ B, const uint16_t* __restrict__ a2tab, int bd,
+                                       unsigned scale) {
+    constexpr int n = (2 * RAD + 1) * (2 * RAD + 1);
+    constexpr unsigned recip = ((1 << 12) + n / 2) / n;
+    const int aa = round2i(sum_sq, 2 * (bd - 8));
+    const int d = round2i(sum, bd - 8);
+    const int p = max(aa * n - d * d, 0);
+    const unsigned long long zz = ((unsigned long long)(unsigned)p * scale + (1u << 19)) >> 20;
+    const int a2 = a2tab[zz > 255 ? 255 : (int)zz];
+    const unsigned b = ((unsigned)(256 - a2) * (unsigned)sum * recip + (1u << 11)) >> 12;
+    A[ar * kBox + bc] = (uint16_t)a2;
+    B[ar * kBox + bc] = (int)b;
+}
+
+// Box sums around every box position (br, bc) -- box rows y_lo-1+br (only
+// those of odd y when odd_rows_only), box columns x_lo-1+bc -- and their a2
+// / b terms.  A warp takes whole box rows: its lanes first form the
+// (2 RAD + 1)-row vertical sums (and sums of squares) of 64 columns in the
+// warp's own buffer V -- two full passes of 32 lanes -- then each box sum of
+// the columns those cover, bc < 64 - 2 RAD, as 2 RAD + 1 of them.  The last
+// few columns of every row (bc >= 64 - 2 RAD) are summed directly afterwards,
+// all rows' together, so no pass over a row runs with most lanes idle.
 template <int RAD>
 __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_t* __restrict__ A,
                                          int32_t* __restrict__ B, const uint16_t* __restrict__ a2tab,
                                          int32_t* __restrict__ V, int R, int C, int y_lo, bool odd_rows_only, int bd,
                                          unsigned scale) {
-    constexpr int n = (2 * RAD + 1) * (2 * RAD + 1);
-    constexpr unsigned recip = ((1 << 12) + n / 2) / n;
+    constexpr int kMain = 64 - 2 * RAD;  // box columns the V buffer covers
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int rows = R + 2, cols = C + 2;
-    const int sh2 = 2 * (bd - 8), sh1 = bd - 8;
+    const int main_cols = min(cols, kMain);
     // Box rows of odd y (= y_lo - 1 + br) are the even br: tiles start on
     // even rows (stripe and unit boundaries are even).
     const int rstep = odd_rows_only ? 2 : 1;
@@ -121,7 +146,7 @@ __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_
         // staged row of box row br is br + 2 (box rows start at y0-1, staged at y0-3)
         const uint16_t* srow = S + (br + 2 - RAD) * kSPitch + (kSOff - 1 - RAD);
         __syncwarp();  // the previous row's sums are consumed
-        for (int cc = lane; cc < cols + 2 * RAD; cc += 32) {
+        for (int cc = lane; cc < main_cols + 2 * RAD; cc += 32) {
             int s = 0, q = 0;
 #pragma unroll
             for (int dy = 0; dy <= 2 * RAD; ++dy) {
@@ -133,22 +158,34 @@ __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_
             V[kVCols + cc] = q;
         }
         __syncwarp();
-        for (int bc = lane; bc < cols; bc += 32) {
+        for (int bc = lane; bc < main_cols; bc += 32) {
             int sum = 0, sum_sq = 0;
 #pragma unroll
             for (int dx = 0; dx <= 2 * RAD; ++dx) {
                 sum += V[bc + dx];
                 sum_sq += V[kVCols + bc + dx];
             }
-            int aa = round2i(sum_sq, sh2);
-            int d = round2i(sum, sh1);
-            int p = max(aa * n - d * d, 0);
-            unsigned long long zz = ((unsigned long long)(unsigned)p * scale + (1u << 19)) >> 20;
-            int a2 = a2tab[zz > 255 ? 255 : (int)zz];
-            unsigned b = ((unsigned)(256 - a2) * (unsigned)sum * recip + (1u << 11)) >> 12;
-            const int ar = odd_rows_only ? br >> 1 : br;  // odd-only rows are stored compactly
-            A[ar * kBox + bc] = (uint16_t)a2;
-            B[ar * kBox + bc] = (int)b;
+            box_ab<RAD>(sum, sum_sq, odd_rows_only ? br >> 1 : br, bc, A, B, a2tab, bd, scale);
+        }
+    }
+    // The remaining box columns [kMain, cols) of every row, summed directly.
+    const int extra = cols - main_cols;  // at most 2 + 2 RAD
+    if (extra > 0) {
+        const int nrows = odd_rows_only ? (rows + 1) >> 1 : rows;
+        for (int i = threadIdx.x; i < nrows * extra; i += kLrThreads) {
+            const int k = i / extra, bc = kMain + (i - k * extra);
+            const int br = odd_rows_only ? 2 * k : k;
+            const uint16_t* box = S + (br + 2 - RAD) * kSPitch + (kSOff - 1 - RAD) + bc;
+            int sum = 0, sum_sq = 0;
+#pragma unroll
+            for (int dy = 0; dy <= 2 * RAD; ++dy)
+#pragma unroll
+                for (int dx = 0; dx <= 2 * RAD; ++dx) {
+                    const int v = box[dy * kSPitch + dx];
+                    sum += v;
+                    sum_sq += v * v;
+                }
+            box_ab<RAD>(sum, sum_sq, k, bc, A, B, a2tab, bd, scale);
         }
     }
 }
