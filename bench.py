@@ -499,41 +499,54 @@ def run_batch(args, world, rank, local):
     from vaco_b200.gpu import Context, DeviceFrame
 
     torch.cuda.set_device(local)
-    frames = []
-    for wl, count in synth.BATCH_MIX:
-        for i in range(count):
-            frames.append(synth.make_frame(wl, synth.seed_for(3, 1000 * rank + len(frames))))
     ctx = Context(local)
     tuning = autotune.load_tuning()
     ctx.set_tuning(**tuning)
-    devs = [DeviceFrame(f, local) for f in frames]
     stream = torch.cuda.current_stream(local)
-    jobs = ctx.batch_jobs(devs)
-    for _ in range(args.warmup):
-        st, _ = ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs)
-        assert all(s == 0 for s in st)
-    torch.cuda.synchronize()
-    launches0 = ctx.launches
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    px = sum(f.output_pixels for f in frames)
-    req = sum(sum(frame_bytes(f)) for f in frames)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm = float(peaks.get("hbm_gbs", 6650.0))
+
+    def time_batch(frames):
+        devs = [DeviceFrame(f, local) for f in frames]
+        jobs = ctx.batch_jobs(devs)
+        for _ in range(args.warmup):
+            st, _ = ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs)
+            assert all(s == 0 for s in st)
+        torch.cuda.synchronize()
+        launches0 = ctx.launches
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        px = sum(f.output_pixels for f in frames)
+        req = sum(sum(frame_bytes(f)) for f in frames)
+        del devs
+        return {"value": round(px / (ms / 1e3) / 1e6, 1), "ms_per_batch": round(ms, 4), "frames_per_batch": len(frames),
+                "hbm_roofline": {"required_bytes_per_batch": int(req),
+                                 "achieved_gbs": round(req / (ms / 1e3) / 1e9, 1), "peak": hbm,
+                                 "frac": round(req / (ms / 1e3) / 1e9 / hbm, 4)},
+                "gpu_launches_per_batch": (ctx.launches - launches0) / max(1, args.steps)}
+
+    mix = []
+    for wl, count in synth.BATCH_MIX:
+        for i in range(count):
+            mix.append(synth.make_frame(wl, synth.seed_for(3, 1000 * rank + len(mix))))
+    mixed = time_batch(mix)
+    del mix
+    # The batched path on 4K 10-bit frames alone (16 per batch).
+    k4 = [synth.make_frame(synth.CONFIG1, synth.seed_for(3, 1000 * rank + 500 + i)) for i in range(16)]
+    only4k = time_batch(k4)
     if rank == 0:
         print(json.dumps({
             "metric": "AV1 post-filter Mpixel/s, batched mixed-resolution frames", "mode": "batch",
-            "value": round(px / (ms / 1e3) / 1e6, 1), "unit": "Mpixel/s", "ms_per_batch": round(ms, 4),
-            "frames_per_batch": len(frames), "steps": args.steps, "warmup": args.warmup,
+            "value": mixed["value"], "unit": "Mpixel/s", "ms_per_batch": mixed["ms_per_batch"],
+            "frames_per_batch": mixed["frames_per_batch"], "steps": args.steps, "warmup": args.warmup,
             "config": {"workload": "batch_mix_64", "mix": [[w.name, c] for w, c in synth.BATCH_MIX], "tuning": tuning},
-            "hbm_roofline": {"required_bytes_per_batch": int(req), "achieved_gbs": round(req / (ms / 1e3) / 1e9, 1),
-                             "peak": hbm, "frac": round(req / (ms / 1e3) / 1e9 / hbm, 4)},
-            "gpu_launches_per_batch": (ctx.launches - launches0) / max(1, args.steps),
+            "hbm_roofline": mixed["hbm_roofline"], "gpu_launches_per_batch": mixed["gpu_launches_per_batch"],
+            "batch_4k_10bit_16": only4k,
         }), flush=True)
     ctx.close()
 
