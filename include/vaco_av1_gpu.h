@@ -469,6 +469,22 @@ VACO_AV1_API int32_t vaco_av1_server_upload(vaco_av1_server* server, int32_t str
 VACO_AV1_API int32_t vaco_av1_server_download(vaco_av1_server* server, int32_t stream_id, int32_t slot,
                                               const vaco_av1_picture* host);
 
+/* Pipelined form of vaco_av1_postfilter_frame_host (no counterpart in vaco,
+ * whose decode_frame filters one frame at a time).  submit validates the
+ * job, enqueues the copy of its inputs to the device, the chain and the copy
+ * of the output planes back to job->dst, and returns a ticket at once; up to
+ * three frames are in flight, each in its own device buffers, so one
+ * frame's copies overlap another's filtering.  A fourth submit before any
+ * wait returns VACO_AV1_LIMIT_EXCEEDED / VACO_AV1_MSG_QUEUE_FULL.  wait
+ * blocks until the frame's output planes are in host memory and returns its
+ * status as vaco_av1_postfilter_frame_host would.  The job's host buffers
+ * must stay valid until its wait returns; page-locked buffers let the
+ * copies run asynchronously.  Host-side check failures are returned by
+ * submit itself. */
+VACO_AV1_API int32_t vaco_av1_postfilter_frame_host_submit(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job,
+                                                           uint64_t* ticket, int32_t* msg);
+VACO_AV1_API int32_t vaco_av1_postfilter_frame_host_wait(vaco_av1_ctx* ctx, uint64_t ticket, int32_t* msg);
+
 /* ---------------------------------------------------------------- frame emission */
 
 /* Destination planes of an emitted frame (Y, U, V; U and V unused for

@@ -20,6 +20,8 @@ SIGNATURES = [
     ("vaco_av1_ctx_destroy", None, [_vp]),
     ("vaco_av1_ctx_last_cuda_error", _i32, [_vp]),
     ("vaco_av1_ctx_launch_count", _u64, [_vp]),
+    ("vaco_av1_postfilter_frame_host_submit", _i32, [_vp, _vp, _vp, _vp]),
+    ("vaco_av1_postfilter_frame_host_wait", _i32, [_vp, _u64, _vp]),
     ("vaco_av1_emit_frame_dev", _i32, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("vaco_av1_emit_frame_host", _i32, [_vp, _vp, _vp, _vp, _vp]),
     ("vaco_av1_postfilter_frame_emit_host", _i32, [_vp, _vp, _vp, _vp]),

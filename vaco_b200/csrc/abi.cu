@@ -312,8 +312,19 @@ void vaco_av1_ctx_destroy(vaco_av1_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (auto& b : ctx->bufs)
-        if (b.p) cudaFree(b.p);
+    for (auto& slot : ctx->pipe)
+        if (slot.done) cudaEventSynchronize(slot.done);
+    for (auto& set : ctx->bufs)
+        for (auto& b : set)
+            if (b.p) cudaFree(b.p);
+    for (auto& slot : ctx->pipe) {
+        for (cudaEvent_t ev : {slot.staged, slot.filtered, slot.done})
+            if (ev) cudaEventDestroy(ev);
+        if (slot.status) cudaFree(slot.status);
+        if (slot.status_host) cudaFreeHost(slot.status_host);
+    }
+    if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+    if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
     if (ctx->status) cudaFree(ctx->status);
     if (ctx->status_host) cudaFreeHost(ctx->status_host);
     for (auto& frame : ctx->marks)
@@ -933,24 +944,28 @@ int32_t vaco_av1_postfilter_frame_dev(vaco_av1_ctx* ctx, void* stream, const vac
 // The chain on a job whose pictures and side information are in host memory:
 // stages the inputs into context scratch, runs the chain into a device
 // picture `*d_out` (context scratch), and leaves the stream synchronized.
+// With sc != s the inputs are copied on stream sc, which `staged` then
+// orders before the chain on s; `defer` is postfilter_dev_impl's.
 static int32_t postfilter_from_host(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_frame_job* job,
-                                    vaco_av1_picture* d_out, int32_t* msg) {
+                                    vaco_av1_picture* d_out, int32_t* msg, cudaStream_t sc = nullptr,
+                                    cudaEvent_t staged = nullptr, bool defer = false) {
+    if (!sc) sc = s;
     const vaco_av1_frame_info& info = job->info;
     const int np = info.monochrome ? 1 : 3;
     const int ssx = info.subsampling_x, ssy = info.subsampling_y;
     cudaError_t e = cudaSuccess;
     vaco_av1_frame_job d = *job;
-    if (!stage_picture_in(ctx, &job->src, np, S_H_IN0, &d.src, s, &e)) return cuda_fail(ctx, e, msg);
+    if (!stage_picture_in(ctx, &job->src, np, S_H_IN0, &d.src, sc, &e)) return cuda_fail(ctx, e, msg);
     if (!alloc_picture(ctx, &job->dst, np, S_H_OUT0, &d.dst, &e)) return cuda_fail(ctx, e, msg);
     size_t n_luma = (size_t)info.mi_rows * info.mi_cols;
     size_t n_chroma = (size_t)((info.mi_rows + ssy) >> ssy) * ((info.mi_cols + ssx) >> ssx);
-    d.tx_luma = stage_array(ctx, S_H_SIDE0, job->tx_luma, n_luma, s, &e);
-    if (e == cudaSuccess) d.tx_chroma = np > 1 ? stage_array(ctx, S_H_SIDE1, job->tx_chroma, n_chroma, s, &e) : nullptr;
-    if (e == cudaSuccess) d.lvl_map = stage_array(ctx, S_H_SIDE2, job->lvl_map, n_luma * 4, s, &e);
-    if (e == cudaSuccess) d.skip = stage_array(ctx, S_H_SIDE3, job->skip, n_luma, s, &e);
+    d.tx_luma = stage_array(ctx, S_H_SIDE0, job->tx_luma, n_luma, sc, &e);
+    if (e == cudaSuccess) d.tx_chroma = np > 1 ? stage_array(ctx, S_H_SIDE1, job->tx_chroma, n_chroma, sc, &e) : nullptr;
+    if (e == cudaSuccess) d.lvl_map = stage_array(ctx, S_H_SIDE2, job->lvl_map, n_luma * 4, sc, &e);
+    if (e == cudaSuccess) d.skip = stage_array(ctx, S_H_SIDE3, job->skip, n_luma, sc, &e);
     if (e == cudaSuccess)
         d.cdef_idx = stage_array(ctx, S_H_SIDE4, job->cdef_idx, (size_t)(job->cdef_count > 0 ? job->cdef_count : 0),
-                                 s, &e);
+                                 sc, &e);
     // All planes' units in one staging buffer.
     size_t total_units = 0;
     for (int k = 0; k < 3; ++k)
@@ -962,7 +977,7 @@ static int32_t postfilter_from_host(vaco_av1_ctx* ctx, cudaStream_t s, const vac
         for (int k = 0; k < 3; ++k) {
             if (job->lr_units[k] && job->lr_unit_count[k] > 0) {
                 e = cudaMemcpyAsync(du + o, job->lr_units[k], sizeof(vaco_av1_lr_unit) * job->lr_unit_count[k],
-                                    cudaMemcpyHostToDevice, s);
+                                    cudaMemcpyHostToDevice, sc);
                 d.lr_units[k] = du + o;
                 o += (size_t)job->lr_unit_count[k];
                 if (e != cudaSuccess) break;
@@ -970,7 +985,12 @@ static int32_t postfilter_from_host(vaco_av1_ctx* ctx, cudaStream_t s, const vac
         }
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
-    int32_t st = postfilter_dev_impl(ctx, s, &d, msg, false);
+    if (sc != s) {
+        e = cudaEventRecord(staged, sc);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, staged, 0);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    }
+    int32_t st = postfilter_dev_impl(ctx, s, &d, msg, defer);
     *d_out = d.dst;
     return st;
 }
@@ -988,6 +1008,76 @@ int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vaco_av1_frame_j
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
     return VACO_AV1_OK;
 }
+// ---------------------------------------------------------------- pipelined host entry points
+
+int32_t vaco_av1_postfilter_frame_host_submit(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job, uint64_t* ticket,
+                                              int32_t* msg) {
+    if (!ctx || !job || !ticket) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    if (!chain_geometry_ok(job)) return invalid(msg, VACO_AV1_MSG_FRAME_GEOMETRY);
+    cudaSetDevice(ctx->device);
+    const int k = (int)(ctx->next_ticket % vaco_av1_ctx::kPipeSlots);
+    vaco_av1_ctx::PipeSlot& slot = ctx->pipe[k];
+    if (slot.busy) {
+        set_msg(msg, VACO_AV1_MSG_QUEUE_FULL);
+        return VACO_AV1_LIMIT_EXCEEDED;
+    }
+    cudaError_t e = cudaSuccess;
+    if (!ctx->copy_in) e = cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !ctx->copy_out) e = cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !slot.done) {
+        e = cudaEventCreateWithFlags(&slot.staged, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.filtered, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaMalloc(&slot.status, sizeof(DeviceStatus));
+        if (e == cudaSuccess) e = cudaMallocHost(&slot.status_host, sizeof(unsigned long long));
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    // The slot's own scratch and status word for this frame.
+    vaco::DeviceStatus* const ctx_status = ctx->status;
+    ctx->scratch_set = 1 + k;
+    ctx->status = slot.status;
+    cudaStream_t s = ctx->stream;
+    e = cudaMemsetAsync(slot.status, 0xFF, sizeof(DeviceStatus), s);
+    vaco_av1_picture dst{};
+    int32_t st = e == cudaSuccess ? postfilter_from_host(ctx, s, job, &dst, msg, ctx->copy_in, slot.staged, true)
+                                  : cuda_fail(ctx, e, msg);
+    if (st == VACO_AV1_OK) {
+        e = cudaEventRecord(slot.filtered, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_out, slot.filtered, 0);
+        if (e == cudaSuccess) e = copy_picture_out(&dst, &job->dst, job->info.monochrome ? 1 : 3, ctx->copy_out);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(slot.status_host, slot.status, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                ctx->copy_out);
+        if (e == cudaSuccess) e = cudaEventRecord(slot.done, ctx->copy_out);
+        if (e != cudaSuccess) st = cuda_fail(ctx, e, msg);
+    }
+    ctx->scratch_set = 0;
+    ctx->status = ctx_status;
+    if (st != VACO_AV1_OK) return st;
+    slot.busy = true;
+    slot.ticket = ctx->next_ticket++;
+    *ticket = slot.ticket;
+    set_msg(msg, VACO_AV1_MSG_NONE);
+    return VACO_AV1_OK;
+}
+
+int32_t vaco_av1_postfilter_frame_host_wait(vaco_av1_ctx* ctx, uint64_t ticket, int32_t* msg) {
+    if (!ctx) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    vaco_av1_ctx::PipeSlot& slot = ctx->pipe[ticket % vaco_av1_ctx::kPipeSlots];
+    if (!slot.busy || slot.ticket != ticket) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    cudaSetDevice(ctx->device);
+    const cudaError_t e = cudaEventSynchronize(slot.done);
+    slot.busy = false;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    const unsigned long long key = *slot.status_host;
+    if (key == kNoError) {
+        set_msg(msg, VACO_AV1_MSG_NONE);
+        return VACO_AV1_OK;
+    }
+    set_msg(msg, (int)(key & 0xFF));
+    return VACO_AV1_INVALID_DATA;
+}
+
 // ---------------------------------------------------------------- frame emission
 
 // The pixel formats pic_to_frame can name (src/decode.rs:3802-3819): every

@@ -66,7 +66,25 @@ struct vaco_av1_ctx {
         void* p = nullptr;
         size_t n = 0;
     };
-    Buf bufs[32];
+    // Scratch sets: 0 for the synchronous entry points, 1 + k for slot k of
+    // the pipelined host entry points (each slot's frame keeps its own
+    // buffers while the next ones are copied in).
+    static constexpr int kPipeSlots = 3;
+    static constexpr int kScratchSets = 1 + kPipeSlots;
+    Buf bufs[kScratchSets][32];
+    int scratch_set = 0;
+
+    // pipelined host entry points (vaco_av1_postfilter_frame_host_submit / _wait)
+    struct PipeSlot {
+        bool busy = false;
+        uint64_t ticket = 0;
+        cudaEvent_t staged = nullptr, filtered = nullptr, done = nullptr;
+        vaco::DeviceStatus* status = nullptr;       // device
+        unsigned long long* status_host = nullptr;  // pinned
+    };
+    PipeSlot pipe[kPipeSlots];
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    uint64_t next_ticket = 1;
 
     // batched form (batch.cu)
     vaco_av1_tuning tuning = {3, 4, 1, 1};
@@ -79,7 +97,7 @@ struct vaco_av1_ctx {
     int sm_count = 0;
 
     void* scratch(int slot, size_t bytes) {
-        Buf& b = bufs[slot];
+        Buf& b = bufs[scratch_set][slot];
         if (b.n >= bytes && b.p) return b.p;
         // Work enqueued without a host sync (deferred status) may still use
         // the old buffer: let it finish before the buffer goes.
