@@ -838,7 +838,10 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
         }
         vaco_av1_picture ucdef, urows;
         if (!alloc_picture(ctx, &out_like, np, S_UCDEF0, &ucdef, &e)) return cuda_fail(ctx, e, msg);
-        SuperresPlane sp[3];
+        // The picture's planes and, for restoration, the pre-CDEF boundary
+        // rows go to one launch.
+        SuperresPlane sp[2 * 3];
+        int nsp = np;
         for (int k = 0; k < np; ++k) {
             const int sx = k ? ssx : 0, sy = k ? ssy : 0;
             sp[k].in = cplane(cdef, k);
@@ -847,25 +850,25 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
             sp[k].output_width = (info.upscaled_width + sx) >> sx;
             sp[k].height = (info.coded_height + sy) >> sy;
         }
-        e = launch_superres(sp, np, info.bit_depth, ctx->status, STAGE_SUPERRES, s);
-        ctx->launches++;
-        if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
         after = ucdef;
         if (lr_active) {
             if (!alloc_picture(ctx, &rows_out_like, np, S_UPRE0, &urows, &e)) return cuda_fail(ctx, e, msg);
             // only the rows the fused kernel wrote (indices 4 .. 4+n)
             for (int k = 0; k < np; ++k) {
                 const int n_rows = pre_rows_written(job->src.height[k], k ? ssy : 0);
-                sp[k].in = DevPlaneC{pre_rows.planes[k] + 4L * pre_rows.stride[k], pre_rows.width[k], n_rows,
-                                     pre_rows.stride[k]};
-                sp[k].out = DevPlane{urows.planes[k] + 4L * urows.stride[k], urows.width[k], n_rows, urows.stride[k]};
-                sp[k].height = n_rows;
+                SuperresPlane& r = sp[np + k];
+                r = sp[k];
+                r.in = DevPlaneC{pre_rows.planes[k] + 4L * pre_rows.stride[k], pre_rows.width[k], n_rows,
+                                 pre_rows.stride[k]};
+                r.out = DevPlane{urows.planes[k] + 4L * urows.stride[k], urows.width[k], n_rows, urows.stride[k]};
+                r.height = n_rows;
             }
-            e = launch_superres(sp, np, info.bit_depth, ctx->status, STAGE_SUPERRES, s);
-            ctx->launches++;
-            if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+            nsp = 2 * np;
             before_rows = urows;
         }
+        e = launch_superres(sp, nsp, info.bit_depth, ctx->status, STAGE_SUPERRES, s);
+        ctx->launches++;
+        if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
     }
     ctx->mark(3, s);
 

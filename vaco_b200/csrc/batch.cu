@@ -363,7 +363,8 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
             const FramePlan& F = plan[i];
             if (r != cudaSuccess || !F.superres) continue;
             const vaco_av1_frame_info& info = jobs[i].info;
-            SuperresPlane sp[3];
+            SuperresPlane sp[2 * 3];
+            int nsp = F.np;
             for (int k = 0; k < F.np; ++k) {
                 const int sx = k ? info.subsampling_x : 0, sy = k ? info.subsampling_y : 0;
                 sp[k].in = dev_cplane(base, F.cdef[k]);
@@ -372,9 +373,8 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
                 sp[k].output_width = (info.upscaled_width + sx) >> sx;
                 sp[k].height = (info.coded_height + sy) >> sy;
             }
-            r = launch_superres(sp, F.np, info.bit_depth, dstatus + i, STAGE_SUPERRES, s);
-            if (r == cudaSuccess && F.lr_active && F.run_lr) {
-                // only the rows the fused kernel wrote (indices 4 .. 4+n)
+            if (F.lr_active && F.run_lr) {
+                // only the rows the fused kernel wrote (indices 4 .. 4+n), in the same launch
                 for (int k = 0; k < F.np; ++k) {
                     const int n_rows = pre_rows_written(jobs[i].src.height[k], k ? info.subsampling_y : 0);
                     DevPlaneC in = dev_cplane(base, F.rows[k]);
@@ -382,12 +382,14 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
                     in.data += 4L * in.stride;
                     out.data += 4L * out.stride;
                     in.height = out.height = n_rows;
-                    sp[k].in = in;
-                    sp[k].out = out;
-                    sp[k].height = n_rows;
+                    sp[F.np + k] = sp[k];
+                    sp[F.np + k].in = in;
+                    sp[F.np + k].out = out;
+                    sp[F.np + k].height = n_rows;
                 }
-                r = launch_superres(sp, F.np, info.bit_depth, dstatus + i, STAGE_SUPERRES, s);
+                nsp = 2 * F.np;
             }
+            r = launch_superres(sp, nsp, info.bit_depth, dstatus + i, STAGE_SUPERRES, s);
         }
         if (r == cudaSuccess && !lr_order.empty() && lr_prefix[lr_order.size()] > 0)
             r = launch_restoration_batch(dtab + off_lr, reinterpret_cast<const int*>(dtab + off_lr_prefix),
@@ -399,7 +401,7 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     };
     // kernel launches of this batch: deblock+CDEF, superres, restoration
     size_t launches = (order.empty() ? 0 : 1) + (lr_order.empty() ? 0 : 1);
-    for (int i : order) launches += plan[i].superres ? (plan[i].lr_active && plan[i].run_lr ? 2 : 1) : 0;
+    for (int i : order) launches += plan[i].superres ? 1 : 0;
     ctx->mark(0, s);
     const bool graphs = ctx->tuning.use_graphs && s != nullptr;
     if (graphs) {

@@ -30,7 +30,9 @@ struct SuperresPlane {
     int output_width;
     int height;
 };
-// Upscales up to 3 planes in one launch (grid.z = plane).
+// Upscales up to kSuperresMaxPlanes planes in one launch (a picture's planes
+// and, for restoration, its pre-CDEF boundary rows).
+constexpr int kSuperresMaxPlanes = 6;
 cudaError_t launch_superres(const SuperresPlane* planes, int count, int bit_depth, DeviceStatus* status,
                             unsigned stage, cudaStream_t stream);
 

@@ -234,7 +234,8 @@ extern "C" int32_t vaco_av1_postfilter_frame_noalloc(void* stream, const vaco_av
     DevPlane* before = pre;
     DevPlane* after = cdef;
     if (host_key == kNoError && superres) {
-        SuperresPlane sp[3];
+        SuperresPlane sp[2 * 3];
+        int nsp = np;
         for (int k = 0; k < np; ++k) {
             const int sx = k ? ssx : 0, sy = k ? ssy : 0;
             sp[k].in = DevPlaneC{cdef[k].data, cdef[k].width, cdef[k].height, cdef[k].stride};
@@ -243,16 +244,17 @@ extern "C" int32_t vaco_av1_postfilter_frame_noalloc(void* stream, const vaco_av
             sp[k].output_width = (info.upscaled_width + sx) >> sx;
             sp[k].height = (info.coded_height + sy) >> sy;
         }
-        e = launch_superres(sp, np, info.bit_depth, status, STAGE_SUPERRES, s);
         after = ucdef;
-        if (e == cudaSuccess && lr_active) {
+        if (lr_active) {  // the pre-CDEF picture too, in the same launch
             for (int k = 0; k < np; ++k) {
-                sp[k].in = DevPlaneC{pre[k].data, pre[k].width, pre[k].height, pre[k].stride};
-                sp[k].out = upre[k];
+                sp[np + k] = sp[k];
+                sp[np + k].in = DevPlaneC{pre[k].data, pre[k].width, pre[k].height, pre[k].stride};
+                sp[np + k].out = upre[k];
             }
-            e = launch_superres(sp, np, info.bit_depth, status, STAGE_SUPERRES, s);
+            nsp = 2 * np;
             before = upre;
         }
+        e = launch_superres(sp, nsp, info.bit_depth, status, STAGE_SUPERRES, s);
         if (e != cudaSuccess) return fail(msg, VACO_AV1_DEVICE_ERROR, VACO_AV1_MSG_CUDA);
     }
 
