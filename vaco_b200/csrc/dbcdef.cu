@@ -160,7 +160,7 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const uint32_t* 
                 taps[2 * k] = word_tap(base_i + f.off[k]);
                 taps[2 * k + 1] = word_tap(base_i - f.off[k]);
             }
-#pragma unroll 2
+#pragma unroll 1  // smaller code: the fused kernel is sensitive to instruction fetch
             for (int j = 0; j < BH / RPI; ++j) {
                 const int woff = j * RPI * PITCH / 2;
                 const uint32_t v = filter_pair<EDGE>(cw[woff], taps, woff, f, pri_on, sec_on);
@@ -173,7 +173,7 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const uint32_t* 
                 taps[2 * k] = pair_tap(t, base_i + f.off[k]);
                 taps[2 * k + 1] = pair_tap(t, base_i - f.off[k]);
             }
-#pragma unroll 2
+#pragma unroll 1  // smaller code: the fused kernel is sensitive to instruction fetch
             for (int j = 0; j < BH / RPI; ++j) {
                 const int woff = j * RPI * PITCH / 2;
                 const uint32_t v = filter_pair<EDGE>(cw[woff], taps, woff, f, pri_on, sec_on);
