@@ -140,6 +140,37 @@ def frame_bytes(f):
     return fin, fout, side
 
 
+def issue_roofline(workload: str, per_stage: dict, clock_info: dict, chain_ms: float, sms: int):
+    """The chain's kernels are integer work that HBM does not bound, so beside
+    the HBM roofline this reports the instruction-issue one: warp
+    instructions per launch (ncu smsp__inst_executed.sum on the same
+    workload, committed in profiles/instructions_per_launch.txt) over the
+    stage's measured launch time, against one warp instruction per SM
+    sub-partition per clock (4 per SM) at the SM clock sampled during the
+    timed region.  None when the workload has no committed counts."""
+    counts = {}
+    tp = ROOT / "profiles" / "instructions_per_launch.txt"
+    if tp.exists():
+        for ln in tp.read_text().splitlines():
+            parts = ln.split()
+            if len(parts) == 3 and not ln.startswith("#") and parts[0] == workload:
+                counts[parts[1]] = int(parts[2])
+    mhz = (clock_info or {}).get("sm_mhz")
+    if not counts or not mhz:
+        return None
+    peak = sms * 4 * mhz * 1e6  # warp instructions per second
+    kernels = {}
+    for stage, n in counts.items():
+        t = per_stage.get(stage, 0.0)
+        if t > 0:
+            kernels[stage] = {"warp_instructions_per_launch": n, "launch_ms": round(t, 5),
+                              "frac": round(n / (t / 1e3) / peak, 4)}
+    total = sum(counts.values())
+    return {"bound": "issue", "unit": "warp instructions/s", "peak": peak, "sms": sms, "sm_mhz": mhz,
+            "kernels": kernels, "chain_frac": round(total / (chain_ms / 1e3) / peak, 4),
+            "source": "ncu smsp__inst_executed.sum per launch (profiles/instructions_per_launch.txt)"}
+
+
 def stage_bytes(f):
     """Algorithmic bytes per launch of each chain kernel (u16 planes).
 
@@ -373,6 +404,8 @@ def run_gpu(args, world, rank, local):
                     traffic = int(parts[2])
         chain_ms = ms / args.steps
         required = fin + fout + side
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        issue = issue_roofline(args.workload, per_stage, clock_info, chain_ms, sms)
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "Mpixel/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(chain_ms, 4),
@@ -399,6 +432,7 @@ def run_gpu(args, world, rank, local):
                                "achieved_gbs": round(required / (chain_ms / 1e3) / 1e9, 1),
                                "frac_of_hbm": round(required / (chain_ms / 1e3) / 1e9 / hbm_peak, 4)},
             "stage_ms": {k: round(v, 5) for k, v in per_stage.items()},
+            "issue_roofline": issue,
             "gpu_launches": int(launches),
             "clocks": clock_info,
         }

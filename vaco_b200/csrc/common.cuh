@@ -80,6 +80,16 @@ __host__ __device__ inline int tx_h_log2(int t) {
 
 inline int div_up(int a, int b) { return (a + b - 1) / b; }
 
+// n / d for 0 <= n < 2^31 and d >= 1 without a division instruction sequence:
+// recip = floor((2^32 - 1) / d) makes umulhi(n, recip) either n / d or one
+// less (the error n / 2^32 stays below one half), and one compare fixes it.
+inline unsigned fast_div_recip(unsigned d) { return 0xFFFFFFFFu / (d ? d : 1u); }
+__device__ __forceinline__ unsigned fast_div(unsigned n, unsigned d, unsigned recip) {
+    unsigned q = __umulhi(n, recip);
+    if ((q + 1) * d <= n) ++q;
+    return q;
+}
+
 // Chroma layouts AV1 can signal (color_config, spec 5.5.2): 4:2:0, 4:2:2 and
 // 4:4:4.  subsampling_y is only coded when subsampling_x is 1, so 4:4:0 does
 // not exist; the fused deblock+CDEF tile layout relies on that.

@@ -40,20 +40,53 @@ constexpr int kSPitch = kMaxTile + 16;  // staged columns x0-8 .. x0+72
 constexpr int kSRows = kMaxTile + 6;    // staged rows y0-3 .. y0+67
 constexpr int kSOff = 8;                // staged column of x0
 constexpr int kBox = kMaxTile + 2;      // box positions y0-1 .. y0+64 (and x)
-constexpr int kPix = kMaxTile * kMaxTile / kLrThreads;  // pixels per thread (16)
 
 // Sgr_Params (radius, epsilon) per set and pass (restoration.rs:286-303).
 __constant__ int8_t c_sgr_r[16][2] = {{2, 1}, {2, 1}, {2, 1}, {2, 1}, {2, 1}, {2, 1}, {2, 1}, {2, 1},
                                       {2, 1}, {2, 1}, {0, 1}, {0, 1}, {0, 1}, {0, 1}, {2, 0}, {2, 0}};
-__constant__ uint8_t c_sgr_e[16][2] = {{12, 4},  {15, 6},  {18, 8},  {21, 9},  {24, 10}, {29, 11},
-                                       {36, 12}, {45, 13}, {56, 14}, {68, 15}, {0, 5},   {0, 8},
-                                       {0, 11},  {0, 14},  {30, 0},  {75, 0}};
+
+struct SgrPassConst {
+    unsigned scale, p_lim;
+};
+struct SgrConstTable {
+    SgrPassConst c[16][2];
+};
+constexpr SgrPassConst sgr_pass_const(int n, int e) {
+    if (e == 0) return SgrPassConst{0, 0};
+    const unsigned n2e = (unsigned)(n * n * e);
+    const unsigned scale = ((1u << 20) + n2e / 2) / n2e;
+    return SgrPassConst{scale, ((1u << 28) - (1u << 19) + scale - 1) / scale};
+}
+constexpr SgrConstTable make_sgr_consts() {
+    constexpr uint8_t e[16][2] = {{12, 4}, {15, 6}, {18, 8}, {21, 9}, {24, 10}, {29, 11}, {36, 12}, {45, 13},
+                                  {56, 14}, {68, 15}, {0, 5},  {0, 8},  {0, 11}, {0, 14}, {30, 0},  {75, 0}};
+    SgrConstTable t{};
+    for (int k = 0; k < 16; ++k) {
+        t.c[k][0] = sgr_pass_const(25, e[k][0]);  // n = 25 samples in a radius-2 box
+        t.c[k][1] = sgr_pass_const(9, e[k][1]);   // n = 9 in a radius-1 box
+    }
+    return t;
+}
+__device__ const SgrConstTable g_sgr_const = make_sgr_consts();
+
+// The a2 table of box_ab: ((z << 8) + z / 2) / (z + 1), with 1 at z = 0 and
+// 256 from z = 255 (restoration.rs:322-328).
+struct alignas(16) A2Table {
+    uint16_t v[256];
+};
+constexpr A2Table make_a2_table() {
+    A2Table t{};
+    for (int z = 0; z < 256; ++z) t.v[z] = (uint16_t)(z >= 255 ? 256 : z == 0 ? 1 : ((z << 8) + z / 2) / (z + 1));
+    return t;
+}
+__device__ const A2Table g_a2 = make_a2_table();
 
 struct LrArgs {
     LrPlane p[3];
     int count;
     int bit_depth;
     int tile_w[3], tile_h[3], tiles_x[3], tiles_y[3], off[3], stripe_h[3];
+    unsigned tiles_x_recip[3], unit_recip[3], stripe_recip[3];  // fast_div_recip of each
     int tile_base[4];
 };
 
@@ -106,17 +139,24 @@ __device__ __forceinline__ bool unit_ok(const vaco_av1_lr_unit& u) {
 // instead of (2 RAD + 1)^2.
 // box_ab's a2 and b (restoration.rs:314-339) from a box sum and sum of
 // squares, stored at box position (ar, bc).
+// A pass's constants for box_ab: scale and p_lim of its set, and the
+// Round2 shifts by 2 (bd - 8) and bd - 8 as (v + half) >> shift.
+struct BoxConst {
+    unsigned scale, p_lim;
+    int sh_sq, half_sq, sh, half;
+};
+
 template <int RAD>
 __device__ __forceinline__ void box_ab(int sum, int sum_sq, int ar, int bc, uint16_t* __restrict__ A,
-                                       int32_t* __restrict__ B, const uint16_t* __restrict__ a2tab, int bd,
-                                       unsigned scale) {
+                                       int32_t* __restrict__ B, const uint16_t* __restrict__ a2tab,
+                                       const BoxConst& k) {
     constexpr int n = (2 * RAD + 1) * (2 * RAD + 1);
     constexpr unsigned recip = ((1 << 12) + n / 2) / n;
-    const int aa = round2i(sum_sq, 2 * (bd - 8));
-    const int d = round2i(sum, bd - 8);
-    const int p = max(aa * n - d * d, 0);
-    const unsigned long long zz = ((unsigned long long)(unsigned)p * scale + (1u << 19)) >> 20;
-    const int a2 = a2tab[zz > 255 ? 255 : (int)zz];
+    const int aa = (sum_sq + k.half_sq) >> k.sh_sq;
+    const int d = (sum + k.half) >> k.sh;
+    const unsigned p = (unsigned)max(aa * n - d * d, 0);
+    const unsigned z = min((min(p, k.p_lim) * k.scale + (1u << 19)) >> 20, 255u);
+    const int a2 = a2tab[z];
     const unsigned b = ((unsigned)(256 - a2) * (unsigned)sum * recip + (1u << 11)) >> 12;
     A[ar * kBox + bc] = (uint16_t)a2;
     B[ar * kBox + bc] = (int)b;
@@ -133,8 +173,8 @@ __device__ __forceinline__ void box_ab(int sum, int sum_sq, int ar, int bc, uint
 template <int RAD>
 __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_t* __restrict__ A,
                                          int32_t* __restrict__ B, const uint16_t* __restrict__ a2tab,
-                                         int32_t* __restrict__ V, int R, int C, int y_lo, bool odd_rows_only, int bd,
-                                         unsigned scale) {
+                                         int32_t* __restrict__ V, int R, int C, int y_lo, bool odd_rows_only,
+                                         const BoxConst& k) {
     constexpr int kMain = 64 - 2 * RAD;  // box columns the V buffer covers
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int rows = R + 2, cols = C + 2;
@@ -165,7 +205,7 @@ __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_
                 sum += V[bc + dx];
                 sum_sq += V[kVCols + bc + dx];
             }
-            box_ab<RAD>(sum, sum_sq, odd_rows_only ? br >> 1 : br, bc, A, B, a2tab, bd, scale);
+            box_ab<RAD>(sum, sum_sq, odd_rows_only ? br >> 1 : br, bc, A, B, a2tab, k);
         }
     }
     // The remaining box columns [kMain, cols) of every row, summed directly.
@@ -173,8 +213,8 @@ __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_
     if (extra > 0) {
         const int nrows = odd_rows_only ? (rows + 1) >> 1 : rows;
         for (int i = threadIdx.x; i < nrows * extra; i += kLrThreads) {
-            const int k = i / extra, bc = kMain + (i - k * extra);
-            const int br = odd_rows_only ? 2 * k : k;
+            const int row = i / extra, bc = kMain + (i - row * extra);
+            const int br = odd_rows_only ? 2 * row : row;
             const uint16_t* box = S + (br + 2 - RAD) * kSPitch + (kSOff - 1 - RAD) + bc;
             int sum = 0, sum_sq = 0;
 #pragma unroll
@@ -185,7 +225,7 @@ __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_
                     sum += v;
                     sum_sq += v * v;
                 }
-            box_ab<RAD>(sum, sum_sq, k, bc, A, B, a2tab, bd, scale);
+            box_ab<RAD>(sum, sum_sq, row, bc, A, B, a2tab, k);
         }
     }
 }
@@ -208,7 +248,7 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     while (pl + 1 < a.count && block >= a.tile_base[pl + 1]) ++pl;
     const LrPlane& P = a.p[pl];
     const int local = block - a.tile_base[pl];
-    const int ty = local / a.tiles_x[pl], tx = local - ty * a.tiles_x[pl];
+    const int ty = (int)fast_div(local, a.tiles_x[pl], a.tiles_x_recip[pl]), tx = local - ty * a.tiles_x[pl];
     const int off = a.off[pl], sh = a.stripe_h[pl];
     const int y_lo = max(ty * a.tile_h[pl] - off, 0);
     const int y_hi = min((ty + 1) * a.tile_h[pl] - off, P.height);
@@ -219,8 +259,8 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     // Unit of this tile (unit_index, restoration.rs:124-133).
-    const int urow = min((y_lo + off) / P.unit_size, P.unit_rows - 1);
-    const int ucol = min(x_lo / P.unit_size, P.unit_cols - 1);
+    const int urow = min((int)fast_div(y_lo + off, P.unit_size, a.unit_recip[pl]), P.unit_rows - 1);
+    const int ucol = min((int)fast_div(x_lo, P.unit_size, a.unit_recip[pl]), P.unit_cols - 1);
     vaco_av1_lr_unit u;
     if (P.copy_only) {
         u.type = VACO_AV1_LR_NONE;
@@ -267,7 +307,7 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     // Stage Source::get (restoration.rs:233-244): rows y_lo-3 .. y_hi+2,
     // columns x_lo-8 .. x_lo+72 as 10 aligned 8-sample vectors per row, all
     // in flight at once by cp.async (edge vectors are gathered sample by sample).
-    const int stripe = (y_lo + off) / sh;
+    const int stripe = (int)fast_div(y_lo + off, sh, a.stripe_recip[pl]);
     const int s_start = stripe * sh - off, s_end = s_start + sh - 1;
     const int srows = R + 6;
     const bool compact = P.before_rows.data != nullptr;
@@ -312,13 +352,25 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
             int a1 = u.vertical[0], b1 = u.vertical[1], c1 = u.vertical[2];
             vv[0] = vv[6] = a1; vv[1] = vv[5] = b1; vv[2] = vv[4] = c1; vv[3] = 128 - 2 * (a1 + b1 + c1);
         }
+        // Horizontal pass: a lane filters two adjacent columns from the 8
+        // samples they share, and stores both as one word (for an odd C the
+        // second value lands in an unused column of the row).
         for (int r = warp; r < srows; r += kWarps) {
             const uint16_t* s = S + r * kSPitch + kSOff - 3;
-            for (int c = lane; c < C; c += 32) {
-                int h = 0;
+            const int c = 2 * lane;  // C <= 64
+            if (c < C) {
+                int v[8];
 #pragma unroll
-                for (int t = 0; t < 7; ++t) h += hv[t] * s[c + t];
-                H[r * kMaxTile + c] = (int16_t)clampi(round2i(h, round_h), -offset, limit - offset);
+                for (int t = 0; t < 8; ++t) v[t] = s[c + t];
+                int h0 = 0, h1 = 0;
+#pragma unroll
+                for (int t = 0; t < 7; ++t) {
+                    h0 += hv[t] * v[t];
+                    h1 += hv[t] * v[t + 1];
+                }
+                h0 = clampi(round2i(h0, round_h), -offset, limit - offset);
+                h1 = clampi(round2i(h1, round_h), -offset, limit - offset);
+                *reinterpret_cast<uint32_t*>(H + r * kMaxTile + c) = (uint32_t)(h0 & 0xFFFF) | ((uint32_t)h1 << 16);
             }
         }
         __syncthreads();
@@ -346,18 +398,20 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     // ---- self-guided (restoration.rs:314-384)
     const int set = min(max((int)u.set, 0), 15);
     const int r0 = c_sgr_r[set][0], r1 = c_sgr_r[set][1];
-    const int e0 = c_sgr_e[set][0], e1 = c_sgr_e[set][1];
-    for (int z = tid; z < 256; z += kLrThreads)
-        a2tab[z] = (uint16_t)(z >= 255 ? 256 : z == 0 ? 1 : ((z << 8) + z / 2) / (z + 1));
+    if (tid < 256 * 2 / 16)
+        reinterpret_cast<uint4*>(a2tab)[tid] = __ldg(reinterpret_cast<const uint4*>(g_a2.v) + tid);
     // Both box passes, into their own buffers, then one final pass.
     __syncthreads();  // a2tab
+    const int sh1 = bd - 8, sh2 = 2 * (bd - 8);
     if (r0 != 0) {
-        const int n2e = 25 * 25 * e0;
-        box_pass<2>(S, A0, B0, a2tab, Vw, R, C, y_lo, true, bd, (unsigned)(((1 << 20) + n2e / 2) / n2e));
+        const SgrPassConst c = g_sgr_const.c[set][0];
+        const BoxConst k{c.scale, c.p_lim, sh2, sh2 ? 1 << (sh2 - 1) : 0, sh1, sh1 ? 1 << (sh1 - 1) : 0};
+        box_pass<2>(S, A0, B0, a2tab, Vw, R, C, y_lo, true, k);
     }
     if (r1 != 0) {
-        const int n2e = 9 * 9 * e1;
-        box_pass<1>(S, A1, B1, a2tab, Vw, R, C, y_lo, false, bd, (unsigned)(((1 << 20) + n2e / 2) / n2e));
+        const SgrPassConst c = g_sgr_const.c[set][1];
+        const BoxConst k{c.scale, c.p_lim, sh2, sh2 ? 1 << (sh2 - 1) : 0, sh1, sh1 ? 1 << (sh1 - 1) : 0};
+        box_pass<1>(S, A1, B1, a2tab, Vw, R, C, y_lo, false, k);
     }
     __syncthreads();
 
@@ -503,6 +557,9 @@ int build_lr_args(const LrPlane* planes, int count, int bit_depth, void* out) {
         a.tile_w[k] = min(planes[k].unit_size, kMaxTile);
         a.tiles_y[k] = div_up(planes[k].height + off, a.tile_h[k]);
         a.tiles_x[k] = div_up(planes[k].width, a.tile_w[k]);
+        a.tiles_x_recip[k] = fast_div_recip((unsigned)a.tiles_x[k]);
+        a.unit_recip[k] = fast_div_recip((unsigned)planes[k].unit_size);
+        a.stripe_recip[k] = fast_div_recip((unsigned)sh);
         a.tile_base[k] = total;
         total += a.tiles_x[k] * a.tiles_y[k];
     }

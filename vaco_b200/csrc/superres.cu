@@ -79,7 +79,7 @@ struct SrPlane {
     SuperresPlane p;
     int step, init;
     int col_blocks;
-    unsigned col_recip;  // floor((2^32 - 1) / col_blocks)
+    unsigned col_recip;  // fast_div_recip(col_blocks)
     int first_block;
     int pairs;           // rows can be read as aligned 32-bit pairs of samples
 };
@@ -113,8 +113,7 @@ __global__ void __launch_bounds__(kSrThreads) superres_kernel(SrArgs a) {
     const SrPlane& S = a.p[k];
     const SuperresPlane& P = S.p;
     const unsigned blk = blk_all - S.first_block;
-    unsigned row_block = __umulhi(blk, S.col_recip);  // floor(blk / col_blocks) or one less
-    if ((row_block + 1) * S.col_blocks <= blk) ++row_block;
+    const unsigned row_block = fast_div(blk, S.col_blocks, S.col_recip);
     const int y0 = row_block * kSrRows;
     const int x_first = (blk - row_block * S.col_blocks) * kSrThreads;
     const int tid = threadIdx.x;
@@ -232,12 +231,12 @@ cudaError_t launch_superres(const SuperresPlane* planes, int count, int bit_dept
                                : 0;
         const int cols = P.output_width > 0 && P.height > 0 ? div_up(P.output_width, kSrThreads) : 0;
         a.p[k].col_blocks = cols > 0 ? cols : 1;
-        a.p[k].col_recip = 0xFFFFFFFFu / (unsigned)a.p[k].col_blocks;
+        a.p[k].col_recip = fast_div_recip((unsigned)a.p[k].col_blocks);
         a.p[k].first_block = (int)blocks;
         a.p[k].pairs = reinterpret_cast<uintptr_t>(P.in.data) % 4 == 0 && P.in.stride % 2 == 0;
         blocks += (long long)cols * (cols > 0 ? div_up(P.height, kSrRows) : 0);
     }
-    if (blocks >= (1LL << 31)) return cudaErrorInvalidValue;  // the in-kernel block split assumes < 2^31
+    if (blocks >= (1LL << 31)) return cudaErrorInvalidValue;  // fast_div needs n < 2^31
     a.count = count;
     a.bit_depth = bit_depth;
     a.status = status;
