@@ -186,26 +186,50 @@ __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_
         // staged row of box row br is br + 2 (box rows start at y0-1, staged at y0-3)
         const uint16_t* srow = S + (br + 2 - RAD) * kSPitch + (kSOff - 1 - RAD);
         __syncwarp();  // the previous row's sums are consumed
-        for (int cc = lane; cc < main_cols + 2 * RAD; cc += 32) {
-            int s = 0, q = 0;
+        {
+            // columns 2 lane and 2 lane + 1 (an odd count computes one
+            // column more, which no box below reads)
+            const int cc = 2 * lane;
+            if (cc < main_cols + 2 * RAD) {
+                int s0 = 0, q0 = 0, s1 = 0, q1 = 0;
 #pragma unroll
-            for (int dy = 0; dy <= 2 * RAD; ++dy) {
-                const int v = srow[dy * kSPitch + cc];
-                s += v;
-                q += v * v;
+                for (int dy = 0; dy <= 2 * RAD; ++dy) {
+                    const int v0 = srow[dy * kSPitch + cc], v1 = srow[dy * kSPitch + cc + 1];
+                    s0 += v0;
+                    q0 += v0 * v0;
+                    s1 += v1;
+                    q1 += v1 * v1;
+                }
+                *reinterpret_cast<int2*>(V + cc) = make_int2(s0, s1);
+                *reinterpret_cast<int2*>(V + kVCols + cc) = make_int2(q0, q1);
             }
-            V[cc] = s;
-            V[kVCols + cc] = q;
         }
         __syncwarp();
-        for (int bc = lane; bc < main_cols; bc += 32) {
-            int sum = 0, sum_sq = 0;
+        {
+            // boxes 2 lane and 2 lane + 1 from one window of 2 RAD + 2
+            // vertical sums
+            const int bc = 2 * lane;
+            if (bc < main_cols) {
+                int vs[2 * RAD + 2], vq[2 * RAD + 2];
 #pragma unroll
-            for (int dx = 0; dx <= 2 * RAD; ++dx) {
-                sum += V[bc + dx];
-                sum_sq += V[kVCols + bc + dx];
+                for (int j = 0; j < RAD + 1; ++j) {
+                    const int2 a = *reinterpret_cast<const int2*>(V + bc + 2 * j);
+                    const int2 b = *reinterpret_cast<const int2*>(V + kVCols + bc + 2 * j);
+                    vs[2 * j] = a.x, vs[2 * j + 1] = a.y;
+                    vq[2 * j] = b.x, vq[2 * j + 1] = b.y;
+                }
+                int sum = 0, sum_sq = 0;
+#pragma unroll
+                for (int dx = 0; dx <= 2 * RAD; ++dx) {
+                    sum += vs[dx];
+                    sum_sq += vq[dx];
+                }
+                const int ar = odd_rows_only ? br >> 1 : br;
+                box_ab<RAD>(sum, sum_sq, ar, bc, A, B, a2tab, k);
+                if (bc + 1 < main_cols)
+                    box_ab<RAD>(sum - vs[0] + vs[2 * RAD + 1], sum_sq - vq[0] + vq[2 * RAD + 1], ar, bc + 1, A, B,
+                                a2tab, k);
             }
-            box_ab<RAD>(sum, sum_sq, odd_rows_only ? br >> 1 : br, bc, A, B, a2tab, k);
         }
     }
     // The remaining box columns [kMain, cols) of every row, summed directly.
