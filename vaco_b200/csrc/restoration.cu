@@ -439,9 +439,10 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     }
     __syncthreads();
 
-    // Pixels of this thread: rows k0 .. k0+7 (k0 = 8 warp) of columns lane
-    // and lane + 32; pixel row k is box row k + 1.  Walking down its rows, a
-    // thread reads each box row of A / B once.
+    // Pixels of this thread: rows k0 .. k0+7 (k0 = 8 warp) of columns 2 lane
+    // and 2 lane + 1; pixel row k is box row k + 1.  Walking down its rows, a
+    // thread reads each box row of A / B once, the four box columns its two
+    // pixels share as two 32-bit (A) and two 64-bit (B) loads.
     //   radius 2 (box rows of odd y only; y_lo is even, so pixel row k0 + j
     //   has odd y when j is odd): with g = 6 A[c] + 5 (A[c-1] + A[c+1]) of a
     //   box row, an odd row takes g of its own box row (shift 8), an even
@@ -451,60 +452,92 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     //   weight 4 on the cross, 3 on the corners.  Likewise for b.
     const int w0 = u.xqd[0], w1 = u.xqd[1];
     const int k0 = 8 * warp;
-    if (k0 >= R) return;
-#pragma unroll 1
-    for (int q = 0; q < 2; ++q) {
-        const int c = lane + 32 * q;
-        if (c >= C) continue;
-        auto g0 = [&](int br, int& ga, int& gb) {  // br even: compact row br / 2
-            const int i = (br >> 1) * kBox + c + 1;
-            ga = 5 * (A0[i - 1] + A0[i + 1]) + 6 * A0[i];
-            gb = 5 * (B0[i - 1] + B0[i + 1]) + 6 * B0[i];
-        };
-        int h3a[3], h3b[3], ca[3], cb[3];
-        auto row1 = [&](int br, int slot) {
-            const int i = br * kBox + c + 1;
-            ca[slot] = A1[i];
-            cb[slot] = B1[i];
-            h3a[slot] = A1[i - 1] + ca[slot] + A1[i + 1];
-            h3b[slot] = B1[i - 1] + cb[slot] + B1[i + 1];
-        };
-        int pa = 0, pb = 0, na = 0, nb = 0;
-        if (r0) g0(k0, pa, pb);
-        if (r1) {
-            row1(k0, 0);
-            row1(k0 + 1, 1);
-        }
+    const int c = 2 * lane;
+    if (k0 >= R || c >= C) return;
+    const bool second = c + 1 < C;
+    // box columns c .. c + 3 of a row (the neighbourhoods of pixels c, c + 1)
+    auto quad = [&](const uint16_t* A, const int32_t* B, int i, int (&qa)[4], int (&qb)[4]) {
+        const uint32_t a01 = *reinterpret_cast<const uint32_t*>(A + i);
+        const uint32_t a23 = *reinterpret_cast<const uint32_t*>(A + i + 2);
+        const int2 b01 = *reinterpret_cast<const int2*>(B + i);
+        const int2 b23 = *reinterpret_cast<const int2*>(B + i + 2);
+        qa[0] = a01 & 0xFFFF, qa[1] = a01 >> 16, qa[2] = a23 & 0xFFFF, qa[3] = a23 >> 16;
+        qb[0] = b01.x, qb[1] = b01.y, qb[2] = b23.x, qb[3] = b23.y;
+    };
+    auto g0 = [&](int br, int (&ga)[2], int (&gb)[2]) {  // br even: compact row br / 2
+        int qa[4], qb[4];
+        quad(A0, B0, (br >> 1) * kBox + c, qa, qb);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int k = k0 + j;
-            const int orig = S[(k + 3) * kSPitch + kSOff + c];
-            int f0 = orig << 4, f1 = orig << 4;
-            if (r0) {
-                if ((j & 1) == 0) {
-                    g0(k + 2, na, nb);
-                    f0 = round2i((pa + na) * orig + (pb + nb), 9);
-                } else {
-                    f0 = round2i(na * orig + nb, 8);
-                    pa = na;
-                    pb = nb;
+        for (int x = 0; x < 2; ++x) {
+            ga[x] = 5 * (qa[x] + qa[x + 2]) + 6 * qa[x + 1];
+            gb[x] = 5 * (qb[x] + qb[x + 2]) + 6 * qb[x + 1];
+        }
+    };
+    int h3a[3][2], h3b[3][2], ca[3][2], cb[3][2];
+    auto row1 = [&](int br, int slot) {
+        int qa[4], qb[4];
+        quad(A1, B1, br * kBox + c, qa, qb);
+#pragma unroll
+        for (int x = 0; x < 2; ++x) {
+            ca[slot][x] = qa[x + 1];
+            cb[slot][x] = qb[x + 1];
+            h3a[slot][x] = qa[x] + qa[x + 1] + qa[x + 2];
+            h3b[slot][x] = qb[x] + qb[x + 1] + qb[x + 2];
+        }
+    };
+    int pa[2] = {0, 0}, pb[2] = {0, 0}, na[2] = {0, 0}, nb[2] = {0, 0};
+    if (r0) g0(k0, pa, pb);
+    if (r1) {
+        row1(k0, 0);
+        row1(k0 + 1, 1);
+    }
+    const bool pair_store = ((P.out.stride | x_lo) & 1) == 0 && (reinterpret_cast<uintptr_t>(P.out.data) & 3) == 0;
+    uint16_t* orow = P.out.data + (long)(y_lo + k0) * P.out.stride + x_lo + c;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int k = k0 + j;
+        const uint32_t ow = *reinterpret_cast<const uint32_t*>(S + (k + 3) * kSPitch + kSOff + c);
+        const int orig[2] = {(int)(ow & 0xFFFF), (int)(ow >> 16)};
+        int f0[2] = {orig[0] << 4, orig[1] << 4}, f1[2] = {orig[0] << 4, orig[1] << 4};
+        if (r0) {
+            if ((j & 1) == 0) {
+                g0(k + 2, na, nb);
+#pragma unroll
+                for (int x = 0; x < 2; ++x) f0[x] = round2i((pa[x] + na[x]) * orig[x] + (pb[x] + nb[x]), 9);
+            } else {
+#pragma unroll
+                for (int x = 0; x < 2; ++x) {
+                    f0[x] = round2i(na[x] * orig[x] + nb[x], 8);
+                    pa[x] = na[x];
+                    pb[x] = nb[x];
                 }
             }
-            if (r1) {
-                row1(k + 2, (j + 2) % 3);
-                const int u_ = j % 3, m_ = (j + 1) % 3, d_ = (j + 2) % 3;
-                const int aa = 4 * h3a[m_] + 3 * (h3a[u_] + h3a[d_]) + ca[u_] + ca[d_];
-                const int bb = 4 * h3b[m_] + 3 * (h3b[u_] + h3b[d_]) + cb[u_] + cb[d_];
-                f1 = round2i(aa * orig + bb, 9);
-            }
-            if (k < R) {
-                const int v = round2i(w0 * f0 + w1 * (orig << 4) + (128 - w0 - w1) * f1, 11);
-                P.out.data[(long)(y_lo + k) * P.out.stride + x_lo + c] = (uint16_t)clampi(v, 0, maxv);
+        }
+        if (r1) {
+            row1(k + 2, (j + 2) % 3);
+            const int u_ = j % 3, m_ = (j + 1) % 3, d_ = (j + 2) % 3;
+#pragma unroll
+            for (int x = 0; x < 2; ++x) {
+                const int aa = 4 * h3a[m_][x] + 3 * (h3a[u_][x] + h3a[d_][x]) + ca[u_][x] + ca[d_][x];
+                const int bb = 4 * h3b[m_][x] + 3 * (h3b[u_][x] + h3b[d_][x]) + cb[u_][x] + cb[d_][x];
+                f1[x] = round2i(aa * orig[x] + bb, 9);
             }
         }
+        if (k < R) {
+            int v[2];
+#pragma unroll
+            for (int x = 0; x < 2; ++x)
+                v[x] = clampi(round2i(w0 * f0[x] + w1 * (orig[x] << 4) + (128 - w0 - w1) * f1[x], 11), 0, maxv);
+            if (pair_store && second) {
+                *reinterpret_cast<uint32_t*>(orow) = (uint32_t)v[0] | ((uint32_t)v[1] << 16);
+            } else {
+                orow[0] = (uint16_t)v[0];
+                if (second) orow[1] = (uint16_t)v[1];
+            }
+        }
+        orow += P.out.stride;
     }
 }
-
 
 __global__ void __launch_bounds__(kLrThreads, 4) restoration_kernel(LrArgs a) { lr_tile(a, blockIdx.x); }
 
