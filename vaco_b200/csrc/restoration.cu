@@ -398,23 +398,40 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
             }
         }
         __syncthreads();
-        // Vertical pass: each thread walks rows 8 warp .. 8 warp + 7 of its
-        // columns, reading each intermediate row once.
+        // Vertical pass: each thread walks rows 8 warp .. 8 warp + 7 of
+        // columns 2 lane and 2 lane + 1, reading each intermediate row once,
+        // both columns as one word.
         const int k0 = 8 * warp;
-        if (k0 >= R) return;
-        for (int c = lane; c < C; c += 32) {
-            int h[14];
+        const int c = 2 * lane;
+        if (k0 >= R || c >= C) return;
+        const bool second = c + 1 < C;
+        const bool pair_store = ((P.out.stride | x_lo) & 1) == 0 && (reinterpret_cast<uintptr_t>(P.out.data) & 3) == 0;
+        int h[14][2];
 #pragma unroll
-            for (int t = 0; t < 14; ++t) h[t] = H[min(k0 + t, kSRows - 1) * kMaxTile + c];
+        for (int t = 0; t < 14; ++t) {
+            const uint32_t w = *reinterpret_cast<const uint32_t*>(H + min(k0 + t, kSRows - 1) * kMaxTile + c);
+            h[t][0] = (int16_t)(w & 0xFFFF);
+            h[t][1] = (int16_t)(w >> 16);
+        }
+        uint16_t* orow = P.out.data + (long)(y_lo + k0) * P.out.stride + x_lo + c;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                if (k0 + j >= R) break;
+        for (int j = 0; j < 8; ++j) {
+            if (k0 + j >= R) break;
+            int v[2];
+#pragma unroll
+            for (int x = 0; x < 2; ++x) {
                 int sum = 0;
 #pragma unroll
-                for (int t = 0; t < 7; ++t) sum += vv[t] * h[j + t];
-                P.out.data[(long)(y_lo + k0 + j) * P.out.stride + x_lo + c] =
-                    (uint16_t)clampi(round2i(sum, 14 - round_h), 0, maxv);
+                for (int t = 0; t < 7; ++t) sum += vv[t] * h[j + t][x];
+                v[x] = clampi(round2i(sum, 14 - round_h), 0, maxv);
             }
+            if (pair_store && second) {
+                *reinterpret_cast<uint32_t*>(orow) = (uint32_t)v[0] | ((uint32_t)v[1] << 16);
+            } else {
+                orow[0] = (uint16_t)v[0];
+                if (second) orow[1] = (uint16_t)v[1];
+            }
+            orow += P.out.stride;
         }
         return;
     }
