@@ -880,10 +880,10 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
             const int sx = k ? ssx : 0, sy = k ? ssy : 0;
             const int w = info.upscaled_width >> sx, h = info.coded_height >> sy;
             if (job->lr_type[k] == VACO_AV1_FRAME_LR_NONE) {
-                // copy_visible_plane (decode.rs:673-681)
-                e = cudaMemcpy2DAsync(job->dst.planes[k], (size_t)job->dst.stride[k] * 2, after.planes[k],
-                                      (size_t)after.stride[k] * 2, (size_t)w * 2, h, cudaMemcpyDeviceToDevice, s);
-                if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+                // copy_visible_plane (decode.rs:673-681), as copy-only tiles
+                // of the same launch: SM copies run at HBM speed, a
+                // device-to-device memcpy at copy-engine speed.
+                lp[nlr++] = copy_only_plane(cplane(after, k), mplane(job->dst, k), w, h, (k && ssy) ? 1 : 0, k);
                 continue;
             }
             if (job->lr_unit_size[k] == 0) {

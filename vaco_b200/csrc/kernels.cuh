@@ -66,6 +66,8 @@ struct LrPlane {
     int plane_index;                // 0 = Y, 1 = U, 2 = V (status-word key of unit checks)
     DeviceStatus* unit_status;      // non-null: validate each tile's unit here (restoration.rs:67-91)
 };
+// A plane whose restoration is off: its tiles only copy `after` into `out`.
+LrPlane copy_only_plane(const DevPlaneC& after, const DevPlane& out, int w, int h, int sub_y, int plane_index);
 // Restores up to 3 planes in one launch.  Units must have been validated.
 cudaError_t launch_restoration(const LrPlane* planes, int count, int bit_depth, cudaStream_t stream);
 // Batched form (see launch_dbcdef_batch): per-frame records of lr_args_size()

@@ -266,10 +266,10 @@ extern "C" int32_t vaco_av1_postfilter_frame_noalloc(void* stream, const vaco_av
             const int sx = k ? ssx : 0, sy = k ? ssy : 0;
             const int w = info.upscaled_width >> sx, h = info.coded_height >> sy;
             const unsigned long long plane_pos = (unsigned long long)k << 44;
-            if (J.lr_type[k] == VACO_AV1_FRAME_LR_NONE) {
-                e = cudaMemcpy2DAsync(J.dst.planes[k], (size_t)J.dst.stride[k] * 2, after[k].data,
-                                      (size_t)after[k].stride * 2, (size_t)w * 2, h, cudaMemcpyDeviceToDevice, s);
-                if (e != cudaSuccess) return fail(msg, VACO_AV1_DEVICE_ERROR, VACO_AV1_MSG_CUDA);
+            if (J.lr_type[k] == VACO_AV1_FRAME_LR_NONE) {  // copy_visible_plane, as copy-only tiles
+                lp[nlr++] = copy_only_plane(DevPlaneC{after[k].data, after[k].width, after[k].height, after[k].stride},
+                                            DevPlane{J.dst.planes[k], w, h, J.dst.stride[k]}, w, h, (k && ssy) ? 1 : 0,
+                                            k);
                 continue;
             }
             const int unit = J.lr_unit_size[k];

@@ -613,6 +613,26 @@ __global__ void range_check_kernel(DevPlaneC p, int w, int h, int maxv, DeviceSt
 
 }  // namespace
 
+// A restoration plane that only copies `after` into `out` (frame-level
+// restoration off for the plane): tiled like a 64-sample unit, no units.
+LrPlane copy_only_plane(const DevPlaneC& after, const DevPlane& out, int w, int h, int sub_y, int plane_index) {
+    LrPlane p{};
+    p.before = DevPlaneC{nullptr, 0, 0, 0};
+    p.before_rows = DevPlaneC{nullptr, 0, 0, 0};
+    p.after = after;
+    p.out = out;
+    p.width = w;
+    p.height = h;
+    p.unit_size = 64;
+    p.sub_y = sub_y;
+    p.units = nullptr;
+    p.unit_cols = p.unit_rows = 1;
+    p.copy_only = 1;
+    p.plane_index = plane_index;
+    p.unit_status = nullptr;
+    return p;
+}
+
 size_t lr_args_size() { return sizeof(LrArgs); }
 
 // Kernel arguments of up to 3 planes; returns the number of tiles.
