@@ -87,7 +87,9 @@ typedef enum vaco_av1_msg {
     VACO_AV1_MSG_QUEUE_FULL = 19,         /* job admission refused */
     VACO_AV1_MSG_TIMEOUT = 20,
     VACO_AV1_MSG_PIXEL_FORMAT = 21,       /* src/decode.rs:3819 */
-    VACO_AV1_MSG_COUNT = 22
+    VACO_AV1_MSG_FG_PARAMS = 22,          /* film grain (no vaco counterpart) */
+    VACO_AV1_MSG_FG_SAMPLE = 23,          /* film grain (no vaco counterpart) */
+    VACO_AV1_MSG_COUNT = 24
 } vaco_av1_msg;
 
 /* Static, NUL-terminated text for a message id ("" for unknown ids). */
@@ -519,6 +521,63 @@ VACO_AV1_API int32_t vaco_av1_emit_frame_host(vaco_av1_ctx* ctx, const vaco_av1_
  * job->dst is ignored. */
 VACO_AV1_API int32_t vaco_av1_postfilter_frame_emit_host(vaco_av1_ctx* ctx, const vaco_av1_frame_job* job,
                                                          const vaco_av1_frame_buffer* out, int32_t* msg);
+
+/* ---------------------------------------------------------------- film grain */
+
+/* film_grain_params() (AV1 spec 5.9.30): the fields vaco's parser reads and
+ * discards (src/frame_header.rs:1125-1210; vaco has no grain synthesis,
+ * src/lib.rs:16-18), plus mc_identity (matrix_coefficients == MC_IDENTITY,
+ * from the sequence header).  Coefficients keep their coded "+128" form. */
+typedef struct vaco_av1_film_grain_params {
+    uint8_t apply_grain;
+    uint8_t num_y_points;             /* 0..14, point values increasing */
+    uint16_t grain_seed;
+    uint8_t point_y_value[14];
+    uint8_t point_y_scaling[14];
+    uint8_t chroma_scaling_from_luma;
+    uint8_t num_cb_points;            /* 0..10 */
+    uint8_t point_cb_value[10];
+    uint8_t point_cb_scaling[10];
+    uint8_t num_cr_points;            /* 0..10 */
+    uint8_t point_cr_value[10];
+    uint8_t point_cr_scaling[10];
+    uint8_t grain_scaling_minus_8;    /* 0..3 */
+    uint8_t ar_coeff_lag;             /* 0..3 */
+    uint8_t ar_coeffs_y_plus_128[24];
+    uint8_t ar_coeffs_cb_plus_128[25];
+    uint8_t ar_coeffs_cr_plus_128[25];
+    uint8_t ar_coeff_shift_minus_6;   /* 0..3 */
+    uint8_t grain_scale_shift;        /* 0..3 */
+    uint8_t cb_mult, cb_luma_mult;
+    uint16_t cb_offset;               /* 0..511 */
+    uint8_t cr_mult, cr_luma_mult;
+    uint16_t cr_offset;               /* 0..511 */
+    uint8_t overlap_flag;
+    uint8_t clip_to_restricted_range;
+    uint8_t mc_identity;
+} vaco_av1_film_grain_params;
+
+/* Film grain synthesis (AV1 spec 7.18.3; the step after the post-filters
+ * that vaco parses but does not implement): `out` = `in` with the grain of
+ * `params` added, for the frame of info->upscaled_width x
+ * info->coded_height (chroma extents rounded up).  `gaussian_sequence` is
+ * the spec's 2048-entry Gaussian_Sequence table in HOST memory, supplied by
+ * the caller (the decoder holds the normative table); the call reads it
+ * before returning.  Fails with VACO_AV1_MSG_FG_PARAMS for parameters
+ * outside the ranges above (point values must increase), with
+ * VACO_AV1_MSG_FRAME_GEOMETRY for planes smaller than the frame, and with
+ * VACO_AV1_MSG_FG_SAMPLE when a sample of `in` exceeds the bit depth.
+ * apply_grain == 0 copies `in` to `out`.  `in` and `out` may not overlap.
+ * _dev: device pointers, runs on `stream` and synchronizes it for the
+ * status.  _host: host pointers, synchronous. */
+VACO_AV1_API int32_t vaco_av1_film_grain_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_picture* in,
+                                             const vaco_av1_picture* out, const vaco_av1_frame_info* info,
+                                             const vaco_av1_film_grain_params* params,
+                                             const int16_t* gaussian_sequence, int32_t* msg);
+VACO_AV1_API int32_t vaco_av1_film_grain_host(vaco_av1_ctx* ctx, const vaco_av1_picture* in,
+                                              const vaco_av1_picture* out, const vaco_av1_frame_info* info,
+                                              const vaco_av1_film_grain_params* params,
+                                              const int16_t* gaussian_sequence, int32_t* msg);
 
 /* The whole chain for callers that cannot call cudaMalloc.  No counterpart in
  * vaco (vaco allocates every intermediate picture through its Budget).

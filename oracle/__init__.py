@@ -50,6 +50,7 @@ def lib():
         l.vo_deblock_picture.argtypes = [vp, vp, vp, vp, vp, vp, vp, i32]
         l.vo_postfilter_frame.argtypes = [vp, i32]
         l.vo_emit_frame.argtypes = [vp, vp, vp]
+        l.vo_film_grain.argtypes = [vp, vp, vp, vp, vp]
         _lib = l
     return _lib
 
@@ -178,3 +179,15 @@ def emit_frame(planes, info: abi.FrameInfo, frame):
         out.linesize[k] = b.shape[1]
     m = lib().vo_emit_frame(C.byref(pic), C.byref(info), C.byref(out))
     return frame, m
+
+
+def film_grain(planes, info: abi.FrameInfo, params: abi.FilmGrainParams, gauss):
+    """Film grain synthesis (AV1 7.18.3) of u16 `planes` with the Gaussian
+    table `gauss` (2048 int16); returns (output planes, msg)."""
+    planes = [_u16(p) for p in planes]
+    outs = [np.zeros_like(p) for p in planes]
+    g = np.ascontiguousarray(gauss, np.int16)
+    pin = picture_struct([ptr(p) for p in planes], [p.shape for p in planes])
+    pout = picture_struct([ptr(o) for o in outs], [o.shape for o in outs])
+    m = lib().vo_film_grain(C.byref(pin), C.byref(pout), C.byref(info), C.byref(params), g.ctypes.data)
+    return outs, m

@@ -12,6 +12,9 @@
 //   deblocking    AV1 spec section 7.14 (vaco has no deblocking filter:
 //                 src/lib.rs:16-18).  Parity of this part is unpinned: no
 //                 vaco code or golden vector exists for it.
+//   film grain    AV1 spec section 7.18.3 (vaco parses the parameters,
+//                 src/frame_header.rs:1125-1210, but has no synthesis).
+//                 Parity unpinned for the same reason.
 //
 // The restated parts are pinned by the dav1d golden vectors vaco checks in
 // (tests/golden/ holds copies; tests/test_oracle_golden.py replays them).
@@ -954,6 +957,292 @@ extern "C" int vo_emit_frame(const vaco_av1_picture* pic, const vaco_av1_frame_i
     return 0;
 }
 
+// ------------------------------------------------------------ film grain
+//
+// AV1 spec 7.18.3 (film grain synthesis), restated step by step: vaco parses
+// the parameters (src/frame_header.rs:1125-1210) but has no synthesis, so
+// this part has no vaco code or golden vector behind it (parity unpinned).
+// The Gaussian sequence is the caller's table.
+
+namespace fg {
+
+struct Grain {
+    const vaco_av1_film_grain_params& p;
+    const int16_t* gauss;
+    int bd, sub_x, sub_y, mono;
+    unsigned reg = 0;
+    int luma[73][82] = {}, cb[73][82] = {}, cr[73][82] = {};
+    int lut[3][256] = {};
+    int grain_min = 0, grain_max = 0;
+
+    Grain(const vaco_av1_film_grain_params& p_, const int16_t* g, int bd_, int sx, int sy, int mono_)
+        : p(p_), gauss(g), bd(bd_), sub_x(sx), sub_y(sy), mono(mono_) {
+        const int center = 128 << (bd - 8);
+        grain_min = -center;
+        grain_max = (256 << (bd - 8)) - 1 - center;
+    }
+
+    static int round2(int x, int n) { return n == 0 ? x : (x + (1 << (n - 1))) >> n; }
+    static int clip3(int lo, int hi, int x) { return x < lo ? lo : x > hi ? hi : x; }
+
+    // 7.18.3.2 random number process
+    int random(int bits) {
+        unsigned r = reg;
+        const unsigned bit = ((r >> 0) ^ (r >> 1) ^ (r >> 3) ^ (r >> 12)) & 1;
+        r = (r >> 1) | (bit << 15);
+        reg = r;
+        return (int)((r >> (16 - bits)) & ((1u << bits) - 1));
+    }
+
+    // 7.18.3.3 generate grain process
+    void generate() {
+        int shift = 12 - bd + p.grain_scale_shift;
+        reg = p.grain_seed;
+        for (int y = 0; y < 73; ++y)
+            for (int x = 0; x < 82; ++x) {
+                const int g = p.num_y_points > 0 ? gauss[random(11)] : 0;
+                luma[y][x] = round2(g, shift);
+            }
+        const int ar_shift = p.ar_coeff_shift_minus_6 + 6;
+        const int lag = p.ar_coeff_lag;
+        for (int y = 3; y < 73; ++y)
+            for (int x = 3; x < 82 - 3; ++x) {
+                int sum = 0, pos = 0;
+                for (int dr = -lag; dr <= 0; ++dr)
+                    for (int dc = -lag; dc <= lag; ++dc) {
+                        if (dr == 0 && dc == 0) break;
+                        sum += luma[y + dr][x + dc] * (p.ar_coeffs_y_plus_128[pos] - 128);
+                        ++pos;
+                    }
+                luma[y][x] = clip3(grain_min, grain_max, luma[y][x] + round2(sum, ar_shift));
+            }
+        if (mono) return;
+        const int cw = sub_x ? 44 : 82, ch = sub_y ? 38 : 73;
+        const bool cb_on = p.num_cb_points || p.chroma_scaling_from_luma;
+        const bool cr_on = p.num_cr_points || p.chroma_scaling_from_luma;
+        reg = p.grain_seed ^ 0xb524u;
+        for (int y = 0; y < ch; ++y)
+            for (int x = 0; x < cw; ++x) cb[y][x] = round2(cb_on ? gauss[random(11)] : 0, shift);
+        reg = p.grain_seed ^ 0x49d8u;
+        for (int y = 0; y < ch; ++y)
+            for (int x = 0; x < cw; ++x) cr[y][x] = round2(cr_on ? gauss[random(11)] : 0, shift);
+        for (int y = 3; y < ch; ++y)
+            for (int x = 3; x < cw - 3; ++x) {
+                int sum0 = 0, sum1 = 0, pos = 0;
+                for (int dr = -lag; dr <= 0; ++dr)
+                    for (int dc = -lag; dc <= lag; ++dc) {
+                        const int c0 = p.ar_coeffs_cb_plus_128[pos] - 128, c1 = p.ar_coeffs_cr_plus_128[pos] - 128;
+                        if (dr == 0 && dc == 0) {
+                            if (p.num_y_points > 0) {
+                                int l = 0;
+                                const int ly = ((y - 3) << sub_y) + 3, lx = ((x - 3) << sub_x) + 3;
+                                for (int i = 0; i <= sub_y; ++i)
+                                    for (int j = 0; j <= sub_x; ++j) l += luma[ly + i][lx + j];
+                                l = round2(l, sub_x + sub_y);
+                                sum0 += l * c0;
+                                sum1 += l * c1;
+                            }
+                            break;
+                        }
+                        sum0 += c0 * cb[y + dr][x + dc];
+                        sum1 += c1 * cr[y + dr][x + dc];
+                        ++pos;
+                    }
+                if (cb_on) cb[y][x] = clip3(grain_min, grain_max, cb[y][x] + round2(sum0, ar_shift));
+                if (cr_on) cr[y][x] = clip3(grain_min, grain_max, cr[y][x] + round2(sum1, ar_shift));
+            }
+    }
+
+    // 7.18.3.4 scaling lookup initialization
+    void init_luts() {
+        for (int plane = 0; plane < (mono ? 1 : 3); ++plane) {
+            const uint8_t *v, *sc;
+            int n;
+            if (plane == 0 || p.chroma_scaling_from_luma) {
+                n = p.num_y_points, v = p.point_y_value, sc = p.point_y_scaling;
+            } else if (plane == 1) {
+                n = p.num_cb_points, v = p.point_cb_value, sc = p.point_cb_scaling;
+            } else {
+                n = p.num_cr_points, v = p.point_cr_value, sc = p.point_cr_scaling;
+            }
+            int* l = lut[plane];
+            if (n == 0) {
+                for (int x = 0; x < 256; ++x) l[x] = 0;
+                continue;
+            }
+            for (int x = 0; x < v[0]; ++x) l[x] = sc[0];
+            for (int i = 0; i < n - 1; ++i) {
+                const int dy = sc[i + 1] - sc[i], dx = v[i + 1] - v[i];
+                const int delta = dy * ((65536 + (dx >> 1)) / dx);
+                for (int x = 0; x < dx; ++x) l[v[i] + x] = sc[i] + ((x * delta + 32768) >> 16);
+            }
+            for (int x = v[n - 1]; x < 256; ++x) l[x] = sc[n - 1];
+        }
+    }
+
+    int scale_lut(int plane, int index) const {
+        const int shift = bd - 8, x = index >> shift, rem = index - (x << shift);
+        if (bd == 8 || x == 255) return lut[plane][x];
+        const int start = lut[plane][x], end = lut[plane][x + 1];
+        return start + round2((end - start) * rem, shift);
+    }
+};
+
+}  // namespace fg
+
+// 7.18.3.5 add noise synthesis process over the whole frame.
+extern "C" int vo_film_grain(const vaco_av1_picture* in, const vaco_av1_picture* out,
+                             const vaco_av1_frame_info* info, const vaco_av1_film_grain_params* p,
+                             const int16_t* gauss) {
+    const int bd = info->bit_depth;
+    const int mono = info->monochrome != 0, sx = info->subsampling_x, sy = info->subsampling_y;
+    const int np = mono ? 1 : 3;
+    if (!(bd == 8 || bd == 10 || bd == 12)) return VACO_AV1_MSG_FG_PARAMS;
+    auto increasing = [](const uint8_t* v, int n) {
+        for (int i = 1; i < n; ++i)
+            if (v[i] <= v[i - 1]) return false;
+        return true;
+    };
+    if (p->num_y_points > 14 || p->num_cb_points > 10 || p->num_cr_points > 10 || p->ar_coeff_lag > 3 ||
+        p->grain_scaling_minus_8 > 3 || p->ar_coeff_shift_minus_6 > 3 || p->grain_scale_shift > 3 ||
+        p->cb_offset > 511 || p->cr_offset > 511 || !increasing(p->point_y_value, p->num_y_points) ||
+        !increasing(p->point_cb_value, p->num_cb_points) || !increasing(p->point_cr_value, p->num_cr_points))
+        return VACO_AV1_MSG_FG_PARAMS;
+    const int w = info->upscaled_width, h = info->coded_height;
+    if (w <= 0 || h <= 0) return VACO_AV1_MSG_FRAME_GEOMETRY;
+    int pw[3], ph[3];
+    for (int k = 0; k < np; ++k) {
+        pw[k] = k ? (w + sx) >> sx : w;
+        ph[k] = k ? (h + sy) >> sy : h;
+        if (in->width[k] < pw[k] || in->height[k] < ph[k] || out->width[k] < pw[k] || out->height[k] < ph[k])
+            return VACO_AV1_MSG_FRAME_GEOMETRY;
+    }
+    const int maxv = (1 << bd) - 1;
+    auto at = [](const vaco_av1_picture* pic, int k, int x, int y) -> uint16_t& {
+        return pic->planes[k][(long)y * pic->stride[k] + x];
+    };
+    for (int k = 0; k < np; ++k)
+        for (int y = 0; y < ph[k]; ++y)
+            for (int x = 0; x < pw[k]; ++x)
+                if (at(in, k, x, y) > maxv) return VACO_AV1_MSG_FG_SAMPLE;
+    if (!p->apply_grain) {
+        for (int k = 0; k < np; ++k)
+            for (int y = 0; y < ph[k]; ++y)
+                for (int x = 0; x < pw[k]; ++x) at(out, k, x, y) = at(in, k, x, y);
+        return 0;
+    }
+    auto* g = new fg::Grain(*p, gauss, bd, sx, sy, mono);
+    g->generate();
+    g->init_luts();
+    // Noise stripes: 34 rows (17 when subsampled) of every plane per stripe of
+    // 32 luma rows; columns up to the last block's reach.
+    const int nstripes = ((h + 1) / 2 + 15) / 16;
+    const int stripe_w = ((w + 1) / 2 + 15) / 16 * 32 + 34;
+    std::vector<int> stripe((size_t)nstripes * 3 * 34 * stripe_w, 0);
+    auto ns = [&](int s, int plane, int i, int x) -> int& {
+        return stripe[(((size_t)s * 3 + plane) * 34 + i) * stripe_w + x];
+    };
+    int luma_num = 0;
+    for (int y = 0; y < (h + 1) / 2; y += 16) {
+        g->reg = p->grain_seed;
+        g->reg ^= ((luma_num * 37 + 178) & 255) << 8;
+        g->reg ^= ((luma_num * 173 + 105) & 255);
+        for (int x = 0; x < (w + 1) / 2; x += 16) {
+            const int rnd = g->random(8);
+            const int off_x = rnd >> 4, off_y = rnd & 15;
+            for (int plane = 0; plane < np; ++plane) {
+                const int psx = plane ? sx : 0, psy = plane ? sy : 0;
+                const int pox = psx ? 6 + off_x : 9 + off_x * 2, poy = psy ? 6 + off_y : 9 + off_y * 2;
+                for (int i = 0; i < (34 >> psy); ++i)
+                    for (int j = 0; j < (34 >> psx); ++j) {
+                        const int(*tmpl)[82] = plane == 0 ? g->luma : plane == 1 ? g->cb : g->cr;
+                        int v = tmpl[poy + i][pox + j];
+                        if (psx == 0) {
+                            if (j < 2 && p->overlap_flag && x > 0) {
+                                const int old = ns(luma_num, plane, i, x * 2 + j);
+                                v = j == 0 ? old * 27 + v * 17 : old * 17 + v * 27;
+                                v = fg::Grain::clip3(g->grain_min, g->grain_max, fg::Grain::round2(v, 5));
+                            }
+                            ns(luma_num, plane, i, x * 2 + j) = v;
+                        } else {
+                            if (j == 0 && p->overlap_flag && x > 0) {
+                                const int old = ns(luma_num, plane, i, x + j);
+                                v = old * 23 + v * 22;
+                                v = fg::Grain::clip3(g->grain_min, g->grain_max, fg::Grain::round2(v, 5));
+                            }
+                            ns(luma_num, plane, i, x + j) = v;
+                        }
+                    }
+            }
+        }
+        ++luma_num;
+    }
+    // Noise image with the vertical overlap, then blending.
+    int min_v, max_luma, max_chroma;
+    if (p->clip_to_restricted_range) {
+        min_v = 16 << (bd - 8);
+        max_luma = 235 << (bd - 8);
+        max_chroma = p->mc_identity ? max_luma : 240 << (bd - 8);
+    } else {
+        min_v = 0;
+        max_luma = max_chroma = (256 << (bd - 8)) - 1;
+    }
+    const int scaling_shift = p->grain_scaling_minus_8 + 8;
+    auto noise = [&](int plane, int y, int x) {
+        const int psy = plane ? sy : 0;
+        const int num = y >> (5 - psy), i = y - (num << (5 - psy));
+        int v = ns(num, plane, i, x);
+        if (psy == 0) {
+            if (i < 2 && num > 0 && p->overlap_flag) {
+                const int old = ns(num - 1, plane, i + 32, x);
+                v = i == 0 ? old * 27 + v * 17 : old * 17 + v * 27;
+                v = fg::Grain::clip3(g->grain_min, g->grain_max, fg::Grain::round2(v, 5));
+            }
+        } else if (i < 1 && num > 0 && p->overlap_flag) {
+            const int old = ns(num - 1, plane, i + 16, x);
+            v = old * 23 + v * 22;
+            v = fg::Grain::clip3(g->grain_min, g->grain_max, fg::Grain::round2(v, 5));
+        }
+        return v;
+    };
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const int orig = at(in, 0, x, y);
+            int v = orig;
+            if (p->num_y_points > 0) {
+                const int n = fg::Grain::round2(g->scale_lut(0, orig) * noise(0, y, x), scaling_shift);
+                v = fg::Grain::clip3(min_v, max_luma, orig + n);
+            }
+            at(out, 0, x, y) = (uint16_t)v;
+        }
+    for (int plane = 1; plane < np; ++plane) {
+        const bool on = (plane == 1 ? p->num_cb_points : p->num_cr_points) > 0 || p->chroma_scaling_from_luma;
+        const int mult = plane == 1 ? p->cb_mult : p->cr_mult, lmult = plane == 1 ? p->cb_luma_mult : p->cr_luma_mult;
+        const int offset = plane == 1 ? p->cb_offset : p->cr_offset;
+        for (int y = 0; y < ph[plane]; ++y)
+            for (int x = 0; x < pw[plane]; ++x) {
+                const int orig = at(in, plane, x, y);
+                int v = orig;
+                if (on) {
+                    const int ly = y << sy, lx = x << sx, lnx = std::min(lx + 1, w - 1);
+                    const int avg = sx ? fg::Grain::round2(at(in, 0, lx, ly) + at(in, 0, lnx, ly), 1) : at(in, 0, lx, ly);
+                    int merged;
+                    if (p->chroma_scaling_from_luma) {
+                        merged = avg;
+                    } else {
+                        const int combined = avg * (lmult - 128) + orig * (mult - 128);
+                        merged = fg::Grain::clip3(0, maxv, (combined >> 6) + ((offset - 256) << (bd - 8)));
+                    }
+                    const int n = fg::Grain::round2(g->scale_lut(plane, merged) * noise(plane, y, x), scaling_shift);
+                    v = fg::Grain::clip3(min_v, max_chroma, orig + n);
+                }
+                at(out, plane, x, y) = (uint16_t)v;
+            }
+    }
+    delete g;
+    return 0;
+}
+
 extern "C" int vo_sizeof(const char* name) {
     struct Entry {
         const char* n;
@@ -970,6 +1259,7 @@ extern "C" int vo_sizeof(const char* name) {
         {"vaco_av1_frame_job", (int)sizeof(vaco_av1_frame_job)},
         {"vaco_av1_tuning", (int)sizeof(vaco_av1_tuning)},
         {"vaco_av1_frame_buffer", (int)sizeof(vaco_av1_frame_buffer)},
+        {"vaco_av1_film_grain_params", (int)sizeof(vaco_av1_film_grain_params)},
     };
     for (const Entry& e : kSizes)
         if (std::strcmp(e.n, name) == 0) return e.s;

@@ -49,6 +49,8 @@ SIGNATURES = [
     ("vaco_av1_ctx_get_tuning", _i32, [_vp, _vp]),
     ("vaco_av1_postfilter_batch_dev", _i32, [_vp, _vp, _vp, _i32, _vp, _vp]),
     ("vaco_av1_postfilter_frame_noalloc", _i32, [_vp, _vp, _pi32]),
+    ("vaco_av1_film_grain_dev", _i32, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _pi32]),
+    ("vaco_av1_film_grain_host", _i32, [_vp, _vp, _vp, _vp, _vp, _vp, _pi32]),
     ("vaco_av1_server_create", _i32, [_vp, _vp]),
     ("vaco_av1_server_destroy", None, [_vp]),
     ("vaco_av1_server_open_stream", _i32, [_vp, _vp, _vp, _i32, _vp, _vp]),

@@ -40,6 +40,8 @@ MESSAGES = {
     19: "job admission refused: queue or memory budget full",
     20: "bounded device wait timed out",
     21: "vaco-codec-av1: unsupported pixel format",
+    22: "invalid AV1 film grain parameters",
+    23: "AV1 film grain sample exceeds bit depth",
 }
 MSG = {
     "NONE": 0, "CDEF_BIT_DEPTH": 1, "CDEF_SAMPLE": 2, "CDEF_BLOCK_PARAMS": 3,
@@ -47,7 +49,7 @@ MSG = {
     "LR_GEOMETRY": 8, "LR_UNIT_COUNT": 9, "LR_COEFFICIENT": 10, "LR_SAMPLE": 11,
     "LR_NO_UNIT_SIZE": 12, "DB_PARAMS": 13, "DB_SAMPLE": 14, "FRAME_GEOMETRY": 15,
     "NULL_ARGUMENT": 16, "CUDA": 17, "SCRATCH_LIMIT": 18, "QUEUE_FULL": 19, "TIMEOUT": 20,
-    "PIXEL_FORMAT": 21,
+    "PIXEL_FORMAT": 21, "FG_PARAMS": 22, "FG_SAMPLE": 23,
 }
 
 LR_NONE, LR_WIENER, LR_SGRPROJ = 0, 1, 2
@@ -168,6 +170,40 @@ class FrameBuffer(C.Structure):
     ]
 
 
+class FilmGrainParams(C.Structure):
+    """vaco_av1_film_grain_params: film_grain_params() of AV1 5.9.30."""
+    _fields_ = [
+        ("apply_grain", C.c_uint8),
+        ("num_y_points", C.c_uint8),
+        ("grain_seed", C.c_uint16),
+        ("point_y_value", C.c_uint8 * 14),
+        ("point_y_scaling", C.c_uint8 * 14),
+        ("chroma_scaling_from_luma", C.c_uint8),
+        ("num_cb_points", C.c_uint8),
+        ("point_cb_value", C.c_uint8 * 10),
+        ("point_cb_scaling", C.c_uint8 * 10),
+        ("num_cr_points", C.c_uint8),
+        ("point_cr_value", C.c_uint8 * 10),
+        ("point_cr_scaling", C.c_uint8 * 10),
+        ("grain_scaling_minus_8", C.c_uint8),
+        ("ar_coeff_lag", C.c_uint8),
+        ("ar_coeffs_y_plus_128", C.c_uint8 * 24),
+        ("ar_coeffs_cb_plus_128", C.c_uint8 * 25),
+        ("ar_coeffs_cr_plus_128", C.c_uint8 * 25),
+        ("ar_coeff_shift_minus_6", C.c_uint8),
+        ("grain_scale_shift", C.c_uint8),
+        ("cb_mult", C.c_uint8),
+        ("cb_luma_mult", C.c_uint8),
+        ("cb_offset", C.c_uint16),
+        ("cr_mult", C.c_uint8),
+        ("cr_luma_mult", C.c_uint8),
+        ("cr_offset", C.c_uint16),
+        ("overlap_flag", C.c_uint8),
+        ("clip_to_restricted_range", C.c_uint8),
+        ("mc_identity", C.c_uint8),
+    ]
+
+
 # numpy structured dtype with the vaco_av1_lr_unit layout (20 bytes)
 def lr_unit_dtype():
     import numpy as np
@@ -198,4 +234,5 @@ STRUCT_SIZES = {
     "vaco_av1_frame_job": C.sizeof(FrameJob),
     "vaco_av1_tuning": C.sizeof(Tuning),
     "vaco_av1_frame_buffer": C.sizeof(FrameBuffer),
+    "vaco_av1_film_grain_params": C.sizeof(FilmGrainParams),
 }

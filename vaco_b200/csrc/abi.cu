@@ -42,6 +42,8 @@ const char* const kMessages[VACO_AV1_MSG_COUNT] = {
     "job admission refused: queue or memory budget full",
     "bounded device wait timed out",
     "vaco-codec-av1: unsupported pixel format",
+    "invalid AV1 film grain parameters",
+    "AV1 film grain sample exceeds bit depth",
 };
 
 unsigned long long make_key(unsigned stage, unsigned long long position, unsigned msg) {
@@ -1196,3 +1198,91 @@ int32_t vaco_av1_postfilter_frame_emit_host(vaco_av1_ctx* ctx, const vaco_av1_fr
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- film grain
+
+// Ranges of film_grain_params() (AV1 5.9.30); point values must increase,
+// which the scaling lookup's divisions rely on.
+static bool grain_params_ok(const vaco_av1_film_grain_params& p) {
+    auto increasing = [](const uint8_t* v, int n) {
+        for (int i = 1; i < n; ++i)
+            if (v[i] <= v[i - 1]) return false;
+        return true;
+    };
+    return p.num_y_points <= 14 && p.num_cb_points <= 10 && p.num_cr_points <= 10 && p.ar_coeff_lag <= 3 &&
+           p.grain_scaling_minus_8 <= 3 && p.ar_coeff_shift_minus_6 <= 3 && p.grain_scale_shift <= 3 &&
+           p.cb_offset <= 511 && p.cr_offset <= 511 && increasing(p.point_y_value, p.num_y_points) &&
+           increasing(p.point_cb_value, p.num_cb_points) && increasing(p.point_cr_value, p.num_cr_points);
+}
+
+// Checks shared by both film grain entry points; returns a message id.
+static int grain_check(const vaco_av1_picture* in, const vaco_av1_picture* out, const vaco_av1_frame_info* info,
+                       const vaco_av1_film_grain_params* params, const int16_t* gauss) {
+    if (!in || !out || !info || !params || !gauss) return VACO_AV1_MSG_NULL_ARGUMENT;
+    if (!bd_valid(info->bit_depth) || !grain_params_ok(*params)) return VACO_AV1_MSG_FG_PARAMS;
+    if (!av1_subsampling_ok(info->subsampling_x, info->subsampling_y)) return VACO_AV1_MSG_FRAME_GEOMETRY;
+    const int w = info->upscaled_width, h = info->coded_height;
+    if (w <= 0 || h <= 0 || w > 65536 || h > 65536) return VACO_AV1_MSG_FRAME_GEOMETRY;
+    const int np = info->monochrome ? 1 : 3;
+    for (int k = 0; k < np; ++k) {
+        const int pw = k ? (w + info->subsampling_x) >> info->subsampling_x : w;
+        const int ph = k ? (h + info->subsampling_y) >> info->subsampling_y : h;
+        if (!in->planes[k] || !out->planes[k]) return VACO_AV1_MSG_NULL_ARGUMENT;
+        if (in->width[k] < pw || in->height[k] < ph || out->width[k] < pw || out->height[k] < ph ||
+            in->stride[k] < in->width[k] || out->stride[k] < out->width[k])
+            return VACO_AV1_MSG_FRAME_GEOMETRY;
+    }
+    return VACO_AV1_MSG_NONE;
+}
+
+static int32_t film_grain_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_picture* in,
+                               const vaco_av1_picture* out, const vaco_av1_frame_info* info,
+                               const vaco_av1_film_grain_params* params, const int16_t* gauss, int32_t* msg) {
+    const int np = info->monochrome ? 1 : 3;
+    const int w = info->upscaled_width, h = info->coded_height;
+    cudaError_t e = reset_status(ctx, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    void* ws = ctx->scratch(S_GRAIN, film_grain_workspace_bytes(np, w, h));
+    if (!ws) return cuda_fail(ctx, cudaErrorMemoryAllocation, msg);
+    DevPlaneC din[3];
+    DevPlane dout[3];
+    for (int k = 0; k < np; ++k) {
+        din[k] = cplane(*in, k);
+        dout[k] = mplane(*out, k);
+    }
+    e = launch_film_grain(*params, gauss, din, dout, np, info->bit_depth, info->subsampling_x, info->subsampling_y,
+                          w, h, ws, ctx->status, ctx->sm_count, s);
+    ctx->launches += params->apply_grain ? 2 : 1;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    return finish(ctx, s, kNoError, msg);
+}
+
+int32_t vaco_av1_film_grain_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_picture* in,
+                                const vaco_av1_picture* out, const vaco_av1_frame_info* info,
+                                const vaco_av1_film_grain_params* params, const int16_t* gaussian_sequence,
+                                int32_t* msg) {
+    if (!ctx) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    if (int m = grain_check(in, out, info, params, gaussian_sequence)) return invalid(msg, m);
+    cudaSetDevice(ctx->device);
+    return film_grain_impl(ctx, (cudaStream_t)stream, in, out, info, params, gaussian_sequence, msg);
+}
+
+int32_t vaco_av1_film_grain_host(vaco_av1_ctx* ctx, const vaco_av1_picture* in, const vaco_av1_picture* out,
+                                 const vaco_av1_frame_info* info, const vaco_av1_film_grain_params* params,
+                                 const int16_t* gaussian_sequence, int32_t* msg) {
+    if (!ctx) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    if (int m = grain_check(in, out, info, params, gaussian_sequence)) return invalid(msg, m);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const int np = info->monochrome ? 1 : 3;
+    vaco_av1_picture din, dout;
+    cudaError_t e = cudaSuccess;
+    if (!stage_picture_in(ctx, in, np, S_H_IN0, &din, s, &e)) return cuda_fail(ctx, e, msg);
+    if (!alloc_picture(ctx, out, np, S_H_OUT0, &dout, &e)) return cuda_fail(ctx, e, msg);
+    const int32_t st = film_grain_impl(ctx, s, &din, &dout, info, params, gaussian_sequence, msg);
+    if (st != VACO_AV1_OK) return st;
+    e = copy_picture_out(&dout, out, np, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    return VACO_AV1_OK;
+}

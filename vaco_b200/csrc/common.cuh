@@ -22,8 +22,9 @@ struct DeviceStatus {
 
 constexpr unsigned long long kNoError = ~0ull;
 
-// Stage numbers order errors across the chain (deblock -> CDEF -> superres -> LR).
-enum Stage : unsigned { STAGE_DEBLOCK = 0, STAGE_CDEF = 1, STAGE_SUPERRES = 2, STAGE_LR = 3 };
+// Stage numbers order errors across the chain (deblock -> CDEF -> superres ->
+// LR), then film grain, which runs on the chain's output.
+enum Stage : unsigned { STAGE_DEBLOCK = 0, STAGE_CDEF = 1, STAGE_SUPERRES = 2, STAGE_LR = 3, STAGE_GRAIN = 4 };
 
 __device__ __forceinline__ void report_error(DeviceStatus* st, unsigned stage,
                                              unsigned long long position, unsigned msg) {

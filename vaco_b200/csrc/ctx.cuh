@@ -126,6 +126,7 @@ enum Slot {
     S_H_SIDE0, S_H_SIDE1, S_H_SIDE2, S_H_SIDE3, S_H_SIDE4, S_H_SIDE5,
     S_BATCH_ARENA, S_BATCH_TABLE,      // batched form: intermediates, per-batch tables
     S_EMIT0, S_EMIT1, S_EMIT2,         // host-entry emission: packed frame planes
+    S_GRAIN,                           // film grain: templates and block offsets
 };
 
 

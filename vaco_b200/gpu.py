@@ -155,6 +155,21 @@ class Context:
         _check(self, st, m)
         return frame
 
+    def film_grain(self, planes: Sequence[np.ndarray], info: abi.FrameInfo, params: abi.FilmGrainParams,
+                   gauss: np.ndarray) -> List[np.ndarray]:
+        """Film grain synthesis through the host entry point: u16 planes in,
+        grained u16 planes out; `gauss` is the 2048-entry Gaussian table."""
+        planes = [np.ascontiguousarray(p, np.uint16) for p in planes]  # alive through the call
+        outs = [np.zeros_like(p) for p in planes]
+        g = np.ascontiguousarray(gauss, np.int16)
+        pin = picture_struct([ptr(p) for p in planes], [p.shape for p in planes])
+        pout = picture_struct([ptr(o) for o in outs], [o.shape for o in outs])
+        m = C.c_int32()
+        st = lib().vaco_av1_film_grain_host(self.handle, C.byref(pin), C.byref(pout), C.byref(info),
+                                            C.byref(params), g.ctypes.data, C.byref(m))
+        _check(self, st, m)
+        return outs
+
     def postfilter_frame_emit(self, f: FrameInputs, fill: int = 0) -> List[np.ndarray]:
         """The chain then pic_to_frame, host arrays in, packed frame out."""
         info = f.info()
