@@ -547,6 +547,104 @@ def run_emit(args, world, rank, local):
                           "unit": "GB/s", "peak": hbm_peak, "lines": lines, "e2e_host": e2e}), flush=True)
 
 
+def grain_params_4k():
+    """Film grain parameters of the grain workload: 8 luma and 4 + 4 chroma
+    scaling points, auto-regression lag 3, overlap on (the most work per
+    sample the syntax allows)."""
+    from vaco_b200 import abi
+
+    rng = np.random.default_rng(0x6A1)
+    p = abi.FilmGrainParams()
+    p.apply_grain, p.grain_seed, p.overlap_flag = 1, 0x1234, 1
+    for n, v, sc in ((8, p.point_y_value, p.point_y_scaling), (4, p.point_cb_value, p.point_cb_scaling),
+                     (4, p.point_cr_value, p.point_cr_scaling)):
+        for i, x in enumerate(np.sort(rng.choice(256, n, replace=False))):
+            v[i], sc[i] = int(x), int(rng.integers(16, 128))
+    p.num_y_points, p.num_cb_points, p.num_cr_points = 8, 4, 4
+    p.grain_scaling_minus_8, p.ar_coeff_lag, p.ar_coeff_shift_minus_6 = 3, 3, 1
+    for arr, n in ((p.ar_coeffs_y_plus_128, 24), (p.ar_coeffs_cb_plus_128, 25), (p.ar_coeffs_cr_plus_128, 25)):
+        for i in range(n):
+            arr[i] = int(np.clip(128 + rng.normal(0, 12), 0, 255))
+    p.cb_mult, p.cb_luma_mult, p.cb_offset = 128, 192, 256
+    p.cr_mult, p.cr_luma_mult, p.cr_offset = 128, 192, 256
+    return p
+
+
+def run_grain(args, world, rank, local):
+    """--mode grain: film grain synthesis (AV1 7.18.3) of 4K 10-bit 4:2:0
+    frames on the device (vaco_av1_film_grain_dev under deferred status, so
+    frames run back to back).  Eight input frames rotate (more than L2
+    holds).  The Gaussian table is a seeded synthetic stand-in for the spec's
+    normative one, which the caller supplies."""
+    import torch
+
+    from vaco_b200 import abi
+    from vaco_b200._lib import lib
+    from vaco_b200.frame import picture_struct
+    from vaco_b200.gpu import Context
+
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    stream = torch.cuda.current_stream(local)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    w, h, bd = 3840, 2160, 10
+    info = abi.FrameInfo()
+    info.bit_depth, info.subsampling_x, info.subsampling_y = bd, 1, 1
+    info.upscaled_width, info.coded_width, info.coded_height = w, w, h
+    info.mi_cols, info.mi_rows = 2 * ((w + 7) >> 3), 2 * ((h + 7) >> 3)
+    shapes = [(h, w), (h // 2, w // 2), (h // 2, w // 2)]
+    gen = torch.Generator(device="cuda").manual_seed(w)
+    gauss = np.random.default_rng(7).integers(-2048, 2048, 2048).astype(np.int16)
+    params = grain_params_4k()
+    frames = []
+    for _ in range(8):
+        src = [torch.randint(0, 1 << bd, s, dtype=torch.int16, device="cuda", generator=gen) for s in shapes]
+        dst = [torch.empty_like(t) for t in src]
+        frames.append((src, dst, picture_struct([t.data_ptr() for t in src], shapes),
+                       picture_struct([t.data_ptr() for t in dst], shapes)))
+    m = C.c_int32()
+    sptr = C.c_void_p(stream.cuda_stream)
+    ctx.set_deferred_status(True)
+
+    def step(i):
+        _, _, pin, pout = frames[i % 8]
+        if lib().vaco_av1_film_grain_dev(ctx.handle, sptr, C.byref(pin), C.byref(pout), C.byref(info),
+                                         C.byref(params), gauss.ctypes.data, C.byref(m)) != abi.OK:
+            raise RuntimeError(f"film grain failed: {abi.MESSAGES.get(m.value)}")
+
+    for i in range(max(args.warmup, 3)):
+        step(i)
+    ctx.flush(stream.cuda_stream)
+    steps = 400
+    launches0 = ctx.launches
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(steps):
+        step(i)
+    e1.record(stream)
+    e1.synchronize()
+    ctx.flush(stream.cuda_stream)
+    ms = e0.elapsed_time(e1) / steps
+    launches = ctx.launches - launches0
+    ctx.set_deferred_status(False)
+    ctx.close()
+    samples = sum(a * b for a, b in shapes)
+    bytes_ = 2 * samples * 2  # u16 planes read once and written once
+    gbs = bytes_ / (ms / 1e3) / 1e9
+    if rank == 0:
+        print(json.dumps({
+            "metric": "AV1 film grain synthesis Mpixel/s on the device", "mode": "grain", "unit": "Mpixel/s",
+            "value": round(w * h / (ms / 1e3) / 1e6, 1), "ms_per_frame": round(ms, 5), "steps": steps,
+            "config": {"workload": "grain_4k_10bit", "width": w, "height": h, "bit_depth": bd, "subsampling": "4:2:0",
+                       "ar_coeff_lag": 3, "overlap": 1, "points": [8, 4, 4], "frames_rotated": 8,
+                       "gaussian_table": "seeded synthetic stand-in (caller-supplied in the product)"},
+            "hbm_roofline": {"bytes_per_frame": bytes_, "achieved_gbs": round(gbs, 1), "peak": hbm_peak,
+                             "frac": round(gbs / hbm_peak, 4)},
+            "gpu_launches": launches}), flush=True)
+
+
 def run_batch(args, world, rank, local):
     """Config 3: 64 frames of mixed sizes (16 each of 640x360 8-bit, 1280x720
     8-bit, 1920x1080 10-bit, 3840x2160 10-bit), independently seeded, through
@@ -618,7 +716,7 @@ def main():
     ap.add_argument("--impl", default="vaco_b200", choices=["vaco_b200", "reference"])
     ap.add_argument("--workload", default="chain_4k_10bit", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--mode", default="headline", choices=["headline", "batch", "serve", "emit"])
+    ap.add_argument("--mode", default="headline", choices=["headline", "batch", "serve", "emit", "grain"])
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="seconds per arrival rate in --mode serve")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -631,6 +729,9 @@ def main():
         return
     if args.mode == "emit":
         run_emit(args, world, rank, local)
+        return
+    if args.mode == "grain":
+        run_grain(args, world, rank, local)
         return
     if args.mode == "serve":
         from vaco_b200 import serve

@@ -110,9 +110,10 @@ VACO_AV1_API int32_t vaco_av1_ctx_last_cuda_error(const vaco_av1_ctx* ctx);
 VACO_AV1_API uint64_t vaco_av1_ctx_launch_count(const vaco_av1_ctx* ctx);
 
 /* Deferred status (no counterpart in vaco, whose calls are synchronous).  By
- * default vaco_av1_postfilter_frame_dev synchronizes its stream before it
- * returns, to report the first error the device found in that frame, as
- * vaco's Result does.  With deferred status enabled it enqueues the chain and
+ * default vaco_av1_postfilter_frame_dev (and vaco_av1_film_grain_dev)
+ * synchronizes its stream before it returns, to report the first error the
+ * device found in that frame, as vaco's Result does.  With deferred status
+ * enabled it enqueues the chain (or the grain) and
  * returns after the host-side checks only, so a decoder can keep frames
  * flowing with no host round trip between them.  Device-side errors then
  * accumulate in the context: vaco_av1_ctx_flush() synchronizes `stream`,
@@ -569,7 +570,9 @@ typedef struct vaco_av1_film_grain_params {
  * VACO_AV1_MSG_FG_SAMPLE when a sample of `in` exceeds the bit depth.
  * apply_grain == 0 copies `in` to `out`.  `in` and `out` may not overlap.
  * _dev: device pointers, runs on `stream` and synchronizes it for the
- * status.  _host: host pointers, synchronous. */
+ * status, unless the context has deferred status enabled (then it only
+ * enqueues; vaco_av1_ctx_flush reports).  _host: host pointers,
+ * synchronous. */
 VACO_AV1_API int32_t vaco_av1_film_grain_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_picture* in,
                                              const vaco_av1_picture* out, const vaco_av1_frame_info* info,
                                              const vaco_av1_film_grain_params* params,

@@ -188,3 +188,47 @@ def test_film_grain_errors_match_oracle(ctx):
     want, _ = oracle.film_grain(planes, info, p, gauss_table())
     got = ctx.film_grain(planes, info, p, gauss_table())
     assert all(np.array_equal(a, b) for a, b in zip(got, want))
+
+
+@pytest.mark.gpu
+def test_film_grain_dev_deferred(oracle_threads):
+    """Under deferred status the device entry point only enqueues; outputs of
+    back-to-back calls are the oracle's, and a sample error surfaces at the
+    flush."""
+    import torch
+
+    from vaco_b200._lib import lib
+    from vaco_b200.frame import picture_struct
+    from vaco_b200.gpu import Context, VacoError
+
+    c = Context(0)
+    c.set_deferred_status(True)
+    try:
+        runs = []
+        for seed in (51, 52, 53):
+            info, planes = frame(seed, 640, 360, 10, "420")
+            if seed == 52:
+                planes[2][10, 20] = 1 << 10  # above the bit depth
+            p = random_params(seed, overlap_flag=1)
+            g = gauss_table(seed)
+            din = [torch.from_numpy(q.view(np.int16)).cuda() for q in planes]
+            dout = [torch.empty_like(t) for t in din]
+            pin = picture_struct([t.data_ptr() for t in din], [q.shape for q in planes])
+            pout = picture_struct([t.data_ptr() for t in dout], [q.shape for q in planes])
+            msg = C.c_int32()
+            st = lib().vaco_av1_film_grain_dev(c.handle, None, C.byref(pin), C.byref(pout), C.byref(info),
+                                               C.byref(p), g.ctypes.data, C.byref(msg))
+            assert st == abi.OK
+            runs.append((info, planes, p, g, dout, din))
+        with pytest.raises(VacoError) as e:
+            c.flush()
+        assert e.value.msg == abi.MSG["FG_SAMPLE"]
+        for info, planes, p, g, dout, _ in (runs[0], runs[2]):
+            want, m = oracle.film_grain(planes, info, p, g)
+            assert m == 0
+            for t, x in zip(dout, want):
+                assert np.array_equal(t.cpu().numpy().view(np.uint16), x)
+        c.flush()
+    finally:
+        c.set_deferred_status(False)
+        c.close()

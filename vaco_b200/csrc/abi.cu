@@ -325,6 +325,12 @@ void vaco_av1_ctx_destroy(vaco_av1_ctx* ctx) {
         if (slot.status) cudaFree(slot.status);
         if (slot.status_host) cudaFreeHost(slot.status_host);
     }
+    for (auto& g : ctx->grain) {
+        if (g.stream) cudaStreamSynchronize(g.stream);
+        for (cudaEvent_t ev : {g.ready, g.free})
+            if (ev) cudaEventDestroy(ev);
+        if (g.stream) cudaStreamDestroy(g.stream);
+    }
     if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
     if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
     if (ctx->status) cudaFree(ctx->status);
@@ -1235,14 +1241,25 @@ static int grain_check(const vaco_av1_picture* in, const vaco_av1_picture* out, 
     return VACO_AV1_MSG_NONE;
 }
 
+// defer: as postfilter_dev_impl's (deferred status: no reset, no sync; the
+// flush reports device-side errors).
 static int32_t film_grain_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_picture* in,
                                const vaco_av1_picture* out, const vaco_av1_frame_info* info,
-                               const vaco_av1_film_grain_params* params, const int16_t* gauss, int32_t* msg) {
+                               const vaco_av1_film_grain_params* params, const int16_t* gauss, int32_t* msg,
+                               bool defer) {
     const int np = info->monochrome ? 1 : 3;
     const int w = info->upscaled_width, h = info->coded_height;
-    cudaError_t e = reset_status(ctx, s);
+    cudaError_t e = defer ? cudaSuccess : reset_status(ctx, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
-    void* ws = ctx->scratch(S_GRAIN, film_grain_workspace_bytes(np, w, h));
+    // The frame's workspace set; its template kernel runs on the set's own
+    // stream once the set's previous reader has run, and `s` waits for it.
+    const int k_set = (int)(ctx->grain_next++ % vaco_av1_ctx::kGrainSets);
+    vaco_av1_ctx::GrainSet& gs = ctx->grain[k_set];
+    if (!gs.stream) e = cudaStreamCreateWithFlags(&gs.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !gs.ready) e = cudaEventCreateWithFlags(&gs.ready, cudaEventDisableTiming);
+    if (e == cudaSuccess && !gs.free) e = cudaEventCreateWithFlags(&gs.free, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    void* ws = ctx->scratch(S_GRAIN0 + k_set, film_grain_workspace_bytes(np, w, h));
     if (!ws) return cuda_fail(ctx, cudaErrorMemoryAllocation, msg);
     DevPlaneC din[3];
     DevPlane dout[3];
@@ -1250,10 +1267,24 @@ static int32_t film_grain_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1
         din[k] = cplane(*in, k);
         dout[k] = mplane(*out, k);
     }
-    e = launch_film_grain(*params, gauss, din, dout, np, info->bit_depth, info->subsampling_x, info->subsampling_y,
-                          w, h, ws, ctx->status, ctx->sm_count, s);
-    ctx->launches += params->apply_grain ? 2 : 1;
+    const int bd = info->bit_depth, ssx = info->subsampling_x, ssy = info->subsampling_y;
+    if (params->apply_grain) {
+        if (gs.used) e = cudaStreamWaitEvent(gs.stream, gs.free, 0);
+        if (e == cudaSuccess) e = launch_grain_template(*params, gauss, np, bd, ssx, ssy, w, h, ws, gs.stream);
+        ctx->launches++;
+        if (e == cudaSuccess) e = cudaEventRecord(gs.ready, gs.stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, gs.ready, 0);
+    }
+    if (e == cudaSuccess) e = launch_grain_apply(*params, din, dout, np, bd, ssx, ssy, w, h, ws, ctx->status,
+                                                 ctx->sm_count, s);
+    ctx->launches++;
+    if (e == cudaSuccess) e = cudaEventRecord(gs.free, s);
+    gs.used = true;
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    if (defer) {
+        set_msg(msg, VACO_AV1_MSG_NONE);
+        return VACO_AV1_OK;
+    }
     return finish(ctx, s, kNoError, msg);
 }
 
@@ -1264,7 +1295,7 @@ int32_t vaco_av1_film_grain_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_
     if (!ctx) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
     if (int m = grain_check(in, out, info, params, gaussian_sequence)) return invalid(msg, m);
     cudaSetDevice(ctx->device);
-    return film_grain_impl(ctx, (cudaStream_t)stream, in, out, info, params, gaussian_sequence, msg);
+    return film_grain_impl(ctx, (cudaStream_t)stream, in, out, info, params, gaussian_sequence, msg, ctx->deferred);
 }
 
 int32_t vaco_av1_film_grain_host(vaco_av1_ctx* ctx, const vaco_av1_picture* in, const vaco_av1_picture* out,
@@ -1279,7 +1310,7 @@ int32_t vaco_av1_film_grain_host(vaco_av1_ctx* ctx, const vaco_av1_picture* in, 
     cudaError_t e = cudaSuccess;
     if (!stage_picture_in(ctx, in, np, S_H_IN0, &din, s, &e)) return cuda_fail(ctx, e, msg);
     if (!alloc_picture(ctx, out, np, S_H_OUT0, &dout, &e)) return cuda_fail(ctx, e, msg);
-    const int32_t st = film_grain_impl(ctx, s, &din, &dout, info, params, gaussian_sequence, msg);
+    const int32_t st = film_grain_impl(ctx, s, &din, &dout, info, params, gaussian_sequence, msg, false);
     if (st != VACO_AV1_OK) return st;
     e = copy_picture_out(&dout, out, np, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

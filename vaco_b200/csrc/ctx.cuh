@@ -71,7 +71,7 @@ struct vaco_av1_ctx {
     // buffers while the next ones are copied in).
     static constexpr int kPipeSlots = 3;
     static constexpr int kScratchSets = 1 + kPipeSlots;
-    Buf bufs[kScratchSets][32];
+    Buf bufs[kScratchSets][40];
     int scratch_set = 0;
 
     // pipelined host entry points (vaco_av1_postfilter_frame_host_submit / _wait)
@@ -85,6 +85,19 @@ struct vaco_av1_ctx {
     PipeSlot pipe[kPipeSlots];
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
     uint64_t next_ticket = 1;
+
+    // film grain (grain.cu): workspace sets whose template kernels run on
+    // their own streams, so the templates of consecutive frames (which depend
+    // only on the parameters) overlap each other and the frames' other work
+    static constexpr int kGrainSets = 4;
+    struct GrainSet {
+        cudaStream_t stream = nullptr;
+        cudaEvent_t ready = nullptr;  // the set's templates are written
+        cudaEvent_t free = nullptr;   // the last apply that read the set has run
+        bool used = false;
+    };
+    GrainSet grain[kGrainSets];
+    uint64_t grain_next = 0;
 
     // batched form (batch.cu)
     vaco_av1_tuning tuning = {3, 4, 1, 1};
@@ -126,7 +139,7 @@ enum Slot {
     S_H_SIDE0, S_H_SIDE1, S_H_SIDE2, S_H_SIDE3, S_H_SIDE4, S_H_SIDE5,
     S_BATCH_ARENA, S_BATCH_TABLE,      // batched form: intermediates, per-batch tables
     S_EMIT0, S_EMIT1, S_EMIT2,         // host-entry emission: packed frame planes
-    S_GRAIN,                           // film grain: templates and block offsets
+    S_GRAIN0, S_GRAIN1, S_GRAIN2, S_GRAIN3,  // film grain workspace sets: templates and block offsets
 };
 
 

@@ -41,10 +41,14 @@ cudaError_t launch_superres(const SuperresPlane* planes, int count, int bit_dept
 // samples from `in` into `out`; `gauss` is the 2048-entry Gaussian table in
 // host memory (copied into the launch).  `workspace` holds
 // film_grain_workspace_bytes(np, w, h) bytes.
+// launch_grain_template fills the workspace from the parameters alone;
+// launch_grain_apply reads it.
 size_t film_grain_workspace_bytes(int np, int w, int h);
-cudaError_t launch_film_grain(const vaco_av1_film_grain_params& p, const int16_t* gauss, const DevPlaneC* in,
-                              const DevPlane* out, int np, int bd, int sub_x, int sub_y, int w, int h,
-                              void* workspace, DeviceStatus* status, int sm_count, cudaStream_t stream);
+cudaError_t launch_grain_template(const vaco_av1_film_grain_params& p, const int16_t* gauss, int np, int bd,
+                                  int sub_x, int sub_y, int w, int h, void* workspace, cudaStream_t stream);
+cudaError_t launch_grain_apply(const vaco_av1_film_grain_params& p, const DevPlaneC* in, const DevPlane* out,
+                               int np, int bd, int sub_x, int sub_y, int w, int h, const void* workspace,
+                               DeviceStatus* status, int sm_count, cudaStream_t stream);
 
 // ---------------------------------------------------------------- frame emission
 // One plane of pic_to_frame / blit (src/decode.rs:3795-3891): `width` x
