@@ -89,7 +89,7 @@ struct vaco_av1_ctx {
     // film grain (grain.cu): workspace sets whose template kernels run on
     // their own streams, so the templates of consecutive frames (which depend
     // only on the parameters) overlap each other and the frames' other work
-    static constexpr int kGrainSets = 4;
+    static constexpr int kGrainSets = 8;
     struct GrainSet {
         cudaStream_t stream = nullptr;
         cudaEvent_t ready = nullptr;  // the set's templates are written
@@ -139,8 +139,11 @@ enum Slot {
     S_H_SIDE0, S_H_SIDE1, S_H_SIDE2, S_H_SIDE3, S_H_SIDE4, S_H_SIDE5,
     S_BATCH_ARENA, S_BATCH_TABLE,      // batched form: intermediates, per-batch tables
     S_EMIT0, S_EMIT1, S_EMIT2,         // host-entry emission: packed frame planes
-    S_GRAIN0, S_GRAIN1, S_GRAIN2, S_GRAIN3,  // film grain workspace sets: templates and block offsets
+    S_GRAIN0,                          // film grain workspace sets S_GRAIN0 .. + kGrainSets - 1
+    S_GRAIN_END = S_GRAIN0 + vaco_av1_ctx::kGrainSets,
 };
+static_assert(S_GRAIN_END <= (int)(sizeof(vaco_av1_ctx::bufs[0]) / sizeof(vaco_av1_ctx::Buf)),
+              "every scratch slot needs a buffer in each set");
 
 
 namespace vaco {

@@ -255,6 +255,7 @@ struct ApplyArgs {
     int bd, sub_x, sub_y, np, w, h, nbx;
     int pw[3], ph[3];
     int chunks_per_row[3];
+    unsigned cpr_recip[3];  // fast_div_recip(chunks_per_row)
     long long chunk_base[4];
     const int16_t* templ;
     const uint8_t* offsets;
@@ -350,9 +351,9 @@ __global__ void __launch_bounds__(kApplyThreads) grain_apply_kernel(const __grid
          c += (long long)gridDim.x * kApplyThreads) {
         int plane = 0;
         while (plane + 1 < a.np && c >= a.chunk_base[plane + 1]) ++plane;
-        const long long j = c - a.chunk_base[plane];
+        const unsigned j = (unsigned)(c - a.chunk_base[plane]);  // < 2^31 (checked on the host)
         const int cpr = a.chunks_per_row[plane];
-        const int y = (int)(j / cpr), x0 = (int)(j - (long long)y * cpr) * 8;
+        const int y = (int)fast_div(j, cpr, a.cpr_recip[plane]), x0 = (int)(j - (unsigned)y * cpr) * 8;
         const int n = min(8, a.pw[plane] - x0);
         const uint16_t* src = a.in[plane].data + (long)y * a.in[plane].stride + x0;
         uint16_t* dst = a.out[plane].data + (long)y * a.out[plane].stride + x0;
@@ -384,10 +385,24 @@ __global__ void __launch_bounds__(kApplyThreads) grain_apply_kernel(const __grid
                 const int mult = plane == 1 ? p.cb_mult : p.cr_mult;
                 const int lmult = plane == 1 ? p.cb_luma_mult : p.cr_luma_mult;
                 const int offset = plane == 1 ? p.cb_offset : p.cr_offset;
+                int lv[16];  // co-located luma, two per chroma sample when subsampled
+                if (full && a.sub_x && 2 * x0 + 16 <= a.w) {
+                    const uint4 q0 = __ldg(reinterpret_cast<const uint4*>(lrow + 2 * x0));
+                    const uint4 q1 = __ldg(reinterpret_cast<const uint4*>(lrow + 2 * x0 + 8));
+                    const uint32_t w8[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) lv[2 * k] = w8[k] & 0xFFFF, lv[2 * k + 1] = w8[k] >> 16;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const int lx = min((x0 + k) << a.sub_x, a.w - 1), lnx = min(lx + 1, a.w - 1);
+                        lv[2 * k] = __ldg(lrow + lx);
+                        lv[2 * k + 1] = __ldg(lrow + lnx);
+                    }
+                }
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    const int lx = min((x0 + k) << a.sub_x, a.w - 1), lnx = min(lx + 1, a.w - 1);
-                    const int avg = a.sub_x ? round2(__ldg(lrow + lx) + __ldg(lrow + lnx), 1) : __ldg(lrow + lx);
+                    const int avg = a.sub_x ? round2(lv[2 * k] + lv[2 * k + 1], 1) : lv[2 * k];
                     merged[k] = p.chroma_scaling_from_luma
                                     ? avg
                                     : clampi(((avg * (lmult - 128) + orig[k] * (mult - 128)) >> 6) +
@@ -479,7 +494,9 @@ cudaError_t launch_grain_apply(const vaco_av1_film_grain_params& p, const DevPla
         a.pw[k] = k ? (w + sub_x) >> sub_x : w;
         a.ph[k] = k ? (h + sub_y) >> sub_y : h;
         a.chunks_per_row[k] = (a.pw[k] + 7) / 8;
+        a.cpr_recip[k] = fast_div_recip((unsigned)a.chunks_per_row[k]);
         a.chunk_base[k] = total;
+        if ((long long)a.chunks_per_row[k] * a.ph[k] >= (1LL << 31)) return cudaErrorInvalidValue;
         total += (long long)a.chunks_per_row[k] * a.ph[k];
     }
     a.chunk_base[np] = total;
