@@ -569,6 +569,10 @@ typedef struct vaco_av1_film_grain_params {
  * VACO_AV1_MSG_FRAME_GEOMETRY for planes smaller than the frame, and with
  * VACO_AV1_MSG_FG_SAMPLE when a sample of `in` exceeds the bit depth.
  * apply_grain == 0 copies `in` to `out`.  `in` and `out` may not overlap.
+ * The grain templates depend only on `params`; they are built on one of the
+ * context's internal streams (one per workspace set, eight sets used in
+ * turn), ordered against `stream` by events, so consecutive frames' template
+ * builds overlap each other and the frames' other work.
  * _dev: device pointers, runs on `stream` and synchronizes it for the
  * status, unless the context has deferred status enabled (then it only
  * enqueues; vaco_av1_ctx_flush reports).  _host: host pointers,
