@@ -60,22 +60,13 @@ struct SideWindow {
     uint32_t lvl[kWinCells];   // loop-filter levels (Yv, Yh, U, V) when a level map is given
 };
 
-// n / d for the few divisors the tile loops meet (segment counts per edge
-// row 9, 10, 17, 18; 16-byte vectors per staged row 6, 10; sentinel window
-// widths 36, 68).  A switch over constants lets the compiler use a multiply
-// for each instead of a general integer division.
-__device__ __forceinline__ int div_small(int n, int d) {
-    switch (d) {
-        case 6: return n / 6;
-        case 9: return n / 9;
-        case 10: return n / 10;
-        case 17: return n / 17;
-        case 18: return n / 18;
-        case 36: return n / 36;
-        case 68: return n / 68;
-        default: return n / d;
-    }
-}
+// n / d for the tile loops' small quotients (segments per edge row 9, 10,
+// 17, 18; 16-byte vectors per staged row 6, 10; sentinel window widths 36,
+// 68) as one multiply and shift: with m = ceil(2^20 / d), (n m) >> 20 is
+// n / d for 0 <= n < 2^20 / d, which every loop here stays under (n is at
+// most 80 x 10, 20 x 18 or 68 x 68).  m is computed once per loop.
+__device__ __forceinline__ unsigned small_div_magic(int d) { return ((1u << 20) + (unsigned)d - 1) / (unsigned)d; }
+__device__ __forceinline__ int small_div(int n, unsigned m) { return (int)(((unsigned)n * m) >> 20); }
 
 struct PlaneGeom {
     int tw, th;        // tile extent in this plane
@@ -240,6 +231,7 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
     const int na0 = PASS == 0 ? gl.th / 4 + 4 : gl.th / 4 + 1, nb0 = PASS == 0 ? gl.tw / 4 + 1 : gl.tw / 4 + 2;
     const int nac = PASS == 0 ? gc.th / 4 + 2 : gc.th / 4 + 1, nbc = PASS == 0 ? gc.tw / 4 + 1 : gc.tw / 4 + 2;
     const int n0 = na0 * nb0, nc = a.num_planes > 1 ? nac * nbc : 0;
+    const unsigned m0 = small_div_magic(nb0), mc = small_div_magic(nbc);
     for (int i = tid; i < n0 + 2 * nc; i += kThreads) {
         int p = 0, j = i;
         if (j >= n0) {
@@ -253,7 +245,7 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
         if (p != 0 && a.levels[1 + p] == 0) continue;
         const PlaneGeom g = p ? gc : gl;
         const int na = p ? nac : na0, nb = p ? nbc : nb0;
-        const int ia = div_small(j, nb), ib = j - ia * nb;
+        const int ia = small_div(j, p ? mc : m0), ib = j - ia * nb;
         const DevPlane& P = a.dst[p];
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
         const int yp = PASS == 0 ? py0 - (p ? 4 : 8) + 4 * ia : py0 + 4 * ia;
@@ -379,8 +371,9 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         uint16_t* t = smem + a.plane_off[p];
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
         const int vpr = g.pitch / 8;
+        const unsigned mv = small_div_magic(vpr);
         for (int v = tid; v < g.rows * vpr; v += kThreads) {
-            const int r = div_small(v, vpr), cv = v - r * vpr;
+            const int r = small_div(v, mv), cv = v - r * vpr;
             const int y = clampi(py0 - kHalo + r, 0, P.height - 1);
             const int x = px0 - kHalo + cv * 8;
             const uint16_t* row = P.data + (long)y * P.stride;
@@ -523,8 +516,9 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         if (px0 + g.tw + 2 <= d.width && py0 + g.th + 2 <= d.height && px0 >= 2 && py0 >= 2) continue;
         uint16_t* t = smem + a.plane_off[p];
         const int wr = g.th + 4, wc = g.tw + 4;
+        const unsigned mw = small_div_magic(wc);
         for (int i = tid; i < wr * wc; i += kThreads) {
-            const int r = div_small(i, wc), c = i - r * wc;
+            const int r = small_div(i, mw), c = i - r * wc;
             const int y = py0 - 2 + r, x = px0 - 2 + c;
             if (y < 0 || x < 0 || y >= d.height || x >= d.width)
                 t[(r + kHalo - 2) * g.pitch + (c + kHalo - 2)] = (uint16_t)kSent;
