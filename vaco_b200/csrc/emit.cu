@@ -25,6 +25,7 @@ struct EmitArgs {
     int two_bytes;
     int vec;
     int chunks_per_row[3];
+    unsigned cpr_recip[3];    // fast_div_recip(chunks_per_row)
     long long chunk_base[4];  // first chunk of each plane; chunk_base[count] = total
 };
 
@@ -41,9 +42,9 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(EmitArgs a) {
         int p = 0;
         while (p + 1 < a.count && i >= a.chunk_base[p + 1]) ++p;
         const EmitPlane& P = a.p[p];
-        const long long j = i - a.chunk_base[p];
+        const unsigned j = (unsigned)(i - a.chunk_base[p]);  // < 2^31 (checked on the host)
         const int cpr = a.chunks_per_row[p];
-        const int y = (int)(j / cpr), x = (int)(j - (long long)y * cpr) * 8;
+        const int y = (int)fast_div(j, cpr, a.cpr_recip[p]), x = (int)(j - (unsigned)y * cpr) * 8;
         const uint16_t* s = P.src + (long)y * P.src_stride + x;
         uint8_t* d = P.dst + (long long)y * P.dst_stride;
         const int n = min(8, P.width - x);
@@ -82,6 +83,8 @@ cudaError_t launch_emit(const EmitPlane* planes, int count, int two_bytes, int s
         const EmitPlane& P = planes[k];
         a.p[k] = P;
         a.chunks_per_row[k] = (P.width + 7) / 8;
+        a.cpr_recip[k] = fast_div_recip((unsigned)(a.chunks_per_row[k] > 0 ? a.chunks_per_row[k] : 1));
+        if ((long long)a.chunks_per_row[k] * P.height >= (1LL << 31)) return cudaErrorInvalidValue;
         a.chunk_base[k] = total;
         total += (long long)a.chunks_per_row[k] * P.height;
         const unsigned dst_align = two_bytes ? 16u : 8u;

@@ -236,8 +236,9 @@ __device__ __forceinline__ void box_pass(const uint16_t* __restrict__ S, uint16_
     const int extra = cols - main_cols;  // at most 2 + 2 RAD
     if (extra > 0) {
         const int nrows = odd_rows_only ? (rows + 1) >> 1 : rows;
+        const unsigned mx = ((1u << 20) + extra - 1) / extra;  // i / extra = (i mx) >> 20 for i < 2^20 / extra
         for (int i = threadIdx.x; i < nrows * extra; i += kLrThreads) {
-            const int row = i / extra, bc = kMain + (i - row * extra);
+            const int row = (int)(((unsigned)i * mx) >> 20), bc = kMain + (i - row * extra);
             const int br = odd_rows_only ? 2 * row : row;
             const uint16_t* box = S + (br + 2 - RAD) * kSPitch + (kSOff - 1 - RAD) + bc;
             int sum = 0, sum_sq = 0;
@@ -306,16 +307,17 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
         const bool vec = ((P.after.stride | P.out.stride) & 7) == 0 &&
                          ((reinterpret_cast<uintptr_t>(P.after.data) | reinterpret_cast<uintptr_t>(P.out.data)) & 15) == 0;
         const int vpr = (C + 7) >> 3;
+        const unsigned mv = ((1u << 20) + vpr - 1) / vpr;  // i / vpr = (i mv) >> 20 for i < 2^20 / vpr
         uint4 q[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            const int i = tid + j * kLrThreads, r = i / vpr, x = x_lo + 8 * (i - r * vpr);
+            const int i = tid + j * kLrThreads, r = (int)(((unsigned)i * mv) >> 20), x = x_lo + 8 * (i - r * vpr);
             if (vec && i < R * vpr && x + 8 <= x_hi)
                 q[j] = __ldg(reinterpret_cast<const uint4*>(P.after.data + (long)(y_lo + r) * P.after.stride + x));
         }
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            const int i = tid + j * kLrThreads, r = i / vpr, x = x_lo + 8 * (i - r * vpr);
+            const int i = tid + j * kLrThreads, r = (int)(((unsigned)i * mv) >> 20), x = x_lo + 8 * (i - r * vpr);
             if (i >= R * vpr) continue;
             uint16_t* dst = P.out.data + (long)(y_lo + r) * P.out.stride + x;
             if (vec && x + 8 <= x_hi) {
