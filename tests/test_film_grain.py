@@ -232,3 +232,43 @@ def test_film_grain_dev_deferred(oracle_threads):
     finally:
         c.set_deferred_status(False)
         c.close()
+
+
+@pytest.mark.gpu
+def test_film_grain_many_frames_in_flight():
+    """Twelve frames back to back under deferred status: more frames than
+    the context has workspace sets, so each set is reused while other frames'
+    templates and grain are still queued.  Every frame must match the oracle."""
+    import torch
+
+    from vaco_b200._lib import lib
+    from vaco_b200.frame import picture_struct
+    from vaco_b200.gpu import Context
+
+    c = Context(0)
+    c.set_deferred_status(True)
+    try:
+        runs = []
+        for seed in range(60, 72):
+            fmt = ("420", "444", "422")[seed % 3]
+            info, planes = frame(seed, 96 + seed, 64 + seed % 7, (8, 10, 12)[seed % 3], fmt)
+            p = random_params(seed, overlap_flag=seed % 2, ar_coeff_lag=seed % 4)
+            g = gauss_table(seed)
+            din = [torch.from_numpy(q.view(np.int16)).cuda() for q in planes]
+            dout = [torch.empty_like(t) for t in din]
+            pin = picture_struct([t.data_ptr() for t in din], [q.shape for q in planes])
+            pout = picture_struct([t.data_ptr() for t in dout], [q.shape for q in planes])
+            msg = C.c_int32()
+            st = lib().vaco_av1_film_grain_dev(c.handle, None, C.byref(pin), C.byref(pout), C.byref(info),
+                                               C.byref(p), g.ctypes.data, C.byref(msg))
+            assert st == abi.OK, abi.MESSAGES.get(msg.value)
+            runs.append((info, planes, p, g, dout, din))
+        c.flush()
+        for info, planes, p, g, dout, _ in runs:
+            want, m = oracle.film_grain(planes, info, p, g)
+            assert m == 0
+            for t, x in zip(dout, want):
+                assert np.array_equal(t.cpu().numpy().view(np.uint16), x)
+    finally:
+        c.set_deferred_status(False)
+        c.close()
