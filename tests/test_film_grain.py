@@ -191,7 +191,7 @@ def test_film_grain_errors_match_oracle(ctx):
 
 
 @pytest.mark.gpu
-def test_film_grain_dev_deferred(oracle_threads):
+def test_film_grain_dev_deferred():
     """Under deferred status the device entry point only enqueues; outputs of
     back-to-back calls are the oracle's, and a sample error surfaces at the
     flush."""
