@@ -96,6 +96,25 @@ def test_oracle_matches_python_restatement(case):
         assert np.array_equal(a, b), f"plane {k}: {int((a != b).sum())} samples differ"
 
 
+@pytest.mark.parametrize("seed", range(300, 316))
+def test_oracle_matches_python_restatement_random(seed):
+    """Sixteen more random cases: format, depth, size and every parameter
+    drawn from the seed."""
+    rng = np.random.default_rng(seed)
+    fmt = ["420", "444", "422", "mono"][seed % 4]
+    bd = [8, 10, 12][int(rng.integers(0, 3))]
+    w, h = int(rng.integers(17, 90)), int(rng.integers(17, 70))
+    info, planes = frame(seed, w, h, bd, fmt)
+    p = random_params(seed, mono=FORMATS[fmt][2])
+    g = gauss_table(seed)
+    got, m = oracle.film_grain(planes, info, p, g)
+    assert m == 0
+    sx, sy, mono = FORMATS[fmt]
+    want = py_film_grain(planes, bd, sx, sy, mono, p, [int(v) for v in g])
+    for k, (a, b) in enumerate(zip(got, want)):
+        assert np.array_equal(a, b), f"plane {k}: {int((a != b).sum())} samples differ"
+
+
 def test_oracle_no_grain_is_a_copy_and_grain_changes_samples():
     info, planes = frame(11, 70, 45, 10, "420")
     p = random_params(11, num_y_points=2)
@@ -134,6 +153,23 @@ def test_film_grain_host_matches_oracle(ctx, case):
     seed, w, h, bd, fmt, over = case
     info, planes = frame(seed, w, h, bd, fmt)
     p = random_params(200 + seed, mono=FORMATS[fmt][2], **over)
+    g = gauss_table(seed)
+    want, m = oracle.film_grain(planes, info, p, g)
+    assert m == 0
+    got = ctx.film_grain(planes, info, p, g)
+    for k, (a, b) in enumerate(zip(got, want)):
+        assert np.array_equal(a, b), f"plane {k}: {int((a != b).sum())} samples differ"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(300, 316))
+def test_film_grain_host_matches_oracle_random(ctx, seed):
+    rng = np.random.default_rng(seed)
+    fmt = ["420", "444", "422", "mono"][seed % 4]
+    bd = [8, 10, 12][int(rng.integers(0, 3))]
+    w, h = int(rng.integers(17, 90)), int(rng.integers(17, 70))
+    info, planes = frame(seed, w, h, bd, fmt)
+    p = random_params(seed, mono=FORMATS[fmt][2])
     g = gauss_table(seed)
     want, m = oracle.film_grain(planes, info, p, g)
     assert m == 0
