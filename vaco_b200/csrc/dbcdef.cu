@@ -614,7 +614,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     }
 }
 
-__global__ void __launch_bounds__(kThreads, 4) dbcdef_kernel(DbCdefArgs a) { dbcdef_tile(a, blockIdx.x, blockIdx.y); }
+__global__ void __launch_bounds__(kThreads, 3) dbcdef_kernel(DbCdefArgs a) { dbcdef_tile(a, blockIdx.x, blockIdx.y); }
 
 // Persistent form: CTAs take tiles of all frames of a batch from a device
 // queue (one atomic per tile), so frames of any size share one launch.
