@@ -32,7 +32,6 @@ import json
 import os
 import pathlib
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -54,6 +53,8 @@ STAGES = ["deblock_cdef", "unused", "superres", "restoration"]  # vaco_av1_ctx_s
 # Per-stage CUDA events go on one frame in STAGE_SAMPLE, spread over the whole
 # timed region, so the events' own stream time barely touches the throughput.
 STAGE_SAMPLE = 8
+E2E_MIN_STEPS = 100          # e2e frames timed at least (each with its H2D and D2H copies)
+SERVED_SECONDS_DEFAULT = 5.0  # seconds per arrival rate and mode in the default line's served block
 
 
 def dist_env():
@@ -65,68 +66,106 @@ def dist_env():
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock, power and clock-event reasons of the benchmarked GPU during
+    the timed region, read in-process through NVML.
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    A thread samples every 2 ms from start() on; mark_start() / mark_end()
+    also take one sample each, right at the edges of the timed region, so a
+    region of a few milliseconds still yields a record made of the samples
+    inside it plus the two bracketing ones.  The GPU is found by the UUID CUDA
+    reports for the device (CUDA_VISIBLE_DEVICES may renumber it), so the
+    sampled GPU is the one the kernels run on.  Falls back to None without
+    NVML."""
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+    REASONS = {"hw_slowdown": "HwSlowdown", "hw_thermal_slowdown": "HwThermalSlowdown",
+               "sw_thermal_slowdown": "SwThermalSlowdown", "sw_power_cap": "SwPowerCap",
+               "hw_power_brake_slowdown": "HwPowerBrakeSlowdown"}
+
+    def __init__(self, cuda_device: int):
+        self.cuda_device = cuda_device
+        self.samples = []  # (time, sm_mhz, reasons bitmask, watts)
+        self.handle = None
+        self.stop_flag = threading.Event()
+        self.t_start = self.t_end = None
+
+    def _open(self):
+        import pynvml as nv
+        import torch
+
+        nv.nvmlInit()
+        props = torch.cuda.get_device_properties(self.cuda_device)
+        try:
+            return nv.nvmlDeviceGetHandleByUUID(f"GPU-{props.uuid}")
+        except Exception:
+            bus = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def sample(self):
+        if self.handle is None:
+            return
+        nv = self.nv
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)
+            reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+            watts = nv.nvmlDeviceGetPowerUsage(self.handle) / 1000.0
+        except Exception:
+            return
+        self.samples.append((time.perf_counter(), sm, reasons, watts))
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
+            import pynvml
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append((time.time(), line.strip()))
+            self.nv = pynvml
+            self.handle = self._open()
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.handle = None
+            return
+
+        def loop():
+            while not self.stop_flag.wait(0.002):
+                self.sample()
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
 
     def mark_start(self):
-        self.t_start = time.time()
+        self.sample()
+        self.t_start = time.perf_counter()
 
     def mark_end(self):
-        self.t_end = time.time()
+        self.t_end = time.perf_counter()
+        self.sample()
 
     def stop(self):
-        if not self.proc:
+        if self.handle is None:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        self.stop_flag.set()
         self.thread.join(timeout=2)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        t0, t1 = getattr(self, "t_start", 0.0), getattr(self, "t_end", float("inf"))
-        timed = [ln for ts, ln in self.lines if t0 <= ts <= t1]
-        if not timed and self.lines:  # region shorter than one sampling period
-            timed = [min(self.lines, key=lambda x: abs(x[0] - (t0 + t1) / 2))[1]]
-        for ln in timed:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 8:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[4:8]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
+        return self.summary()
+
+    def summary(self):
+        """The record of the timed region: samples inside it plus the last
+        one before and the first one after."""
+        t0 = self.t_start if self.t_start is not None else -float("inf")
+        t1 = self.t_end if self.t_end is not None else float("inf")
+        inside = [x for x in self.samples if t0 <= x[0] <= t1]
+        before = [x for x in self.samples if x[0] < t0][-1:]
+        after = [x for x in self.samples if x[0] > t1][:1]
+        window = before + inside + after
+        if not window:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = set()
+        for _, _, mask, _ in window:
+            for name, suffix in self.REASONS.items():
+                bit = getattr(self.nv, "nvmlClocksEventReason" + suffix, 0)
+                if mask & bit:
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(x[1] for x in window), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "power_w_median": round(statistics.median(x[3] for x in window), 1),
+                "samples": len(window), "samples_inside_region": len(inside),
+                "source": "NVML, every 2 ms plus one sample at each edge of the timed region"}
 
 
 # ---------------------------------------------------------------- algorithmic bytes
@@ -197,19 +236,45 @@ def stage_bytes(f):
     }
 
 
+# ---------------------------------------------------------------- frames
+def workload_frames(cfg_idx: int, workload, rank: int, count: int = ROTATE_FRAMES):
+    """The frames rank `rank` of the GPU arm rotates through; the CPU legs
+    filter the same frames (rank 0's)."""
+    from vaco_b200 import replicas
+
+    return [synth.make_frame(workload, s) for s in replicas.frame_seeds(rank, count, cfg_idx)]
+
+
+def band_of(f, rows: int):
+    """The top `rows` luma rows (a multiple of 64) of frame f as a frame of
+    its own: same width, content, side information and restoration units
+    (the first unit rows).  A bounded CPU sample of f's workload."""
+    import dataclasses
+
+    assert rows % 64 == 0 and 0 < rows <= f.coded_height
+    g = dataclasses.replace(f, coded_height=rows)
+    mi_rows = g.mi_rows
+    g.planes = [np.ascontiguousarray(p[: g.padded_shape(k)[0]]) for k, p in enumerate(f.planes)]
+    g.tx_luma = np.ascontiguousarray(f.tx_luma[:mi_rows])
+    g.tx_chroma = np.ascontiguousarray(f.tx_chroma[: (mi_rows + f.subsampling_y) >> f.subsampling_y])
+    g.skip = np.ascontiguousarray(f.skip[:mi_rows])
+    g.cdef_idx = np.ascontiguousarray(f.cdef_idx[: (mi_rows + 15) // 16])
+    g.lvl_map = None if f.lvl_map is None else np.ascontiguousarray(f.lvl_map[:mi_rows])
+    units = []
+    for k, u in enumerate(f.lr_units):
+        h, w = g.output_shape(k)
+        size = f.lr_unit_size[k]
+        cols = max((w + size // 2) // size, 1)
+        urows = max((h + size // 2) // size, 1)
+        units.append(np.ascontiguousarray(u[: urows * cols]))
+    g.lr_units = units
+    return g
+
+
 # ---------------------------------------------------------------- CPU legs
-def cpu_sample_frame(workload, rows):
-    """A bounded sample of the workload: same width, content and parameter
-    model, `rows` luma rows."""
-    w = synth.Workload(workload.name + f"_band{rows}", workload.width, rows, workload.bit_depth,
-                       workload.upscaled_width, workload.chain)
-    return synth.make_frame(w, synth.seed_for(7, rows))
-
-
 def time_oracle(f, threads, repeats):
     import oracle
 
-    oracle.postfilter_frame(f, threads=threads)  # warm (page-in)
     t0 = time.perf_counter()
     for _ in range(repeats):
         _, m = oracle.postfilter_frame(f, threads=threads)
@@ -217,49 +282,67 @@ def time_oracle(f, threads, repeats):
     return (time.perf_counter() - t0) / repeats
 
 
-def cpu_baseline(workload):
-    """Oracle on 1 core on a band of the workload (~10-30 s of CPU work)."""
-    rows = 256
-    f = cpu_sample_frame(workload, rows)
-    t = time_oracle(f, 1, 1)
-    repeats = max(1, min(20, int(12.0 / max(t, 1e-3))))
-    t = time_oracle(f, 1, repeats)
-    return {"value": round(f.output_pixels / t / 1e6, 3), "unit": "Mpixel/s", "cores": 1, "kind": "port",
-            "sample": f"{repeats} x {f.upscaled_width}x{rows} band of {workload.name} (full chain), 1 thread"}
+def cpu_baseline(frames, workload, seconds: float = 12.0):
+    """The oracle on 1 core over the GPU arm's own frames, whole frames one
+    after another until about `seconds` of CPU work (at least one)."""
+    import oracle
+
+    oracle.lib()  # load (page in) outside the timing
+    t0 = time.perf_counter()
+    n, px = 0, 0
+    while n < len(frames) and (n == 0 or time.perf_counter() - t0 < seconds):
+        _, m = oracle.postfilter_frame(frames[n], threads=1)
+        assert m == 0
+        px += frames[n].output_pixels
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": round(px / dt / 1e6, 3), "unit": "Mpixel/s", "cores": 1, "kind": "port",
+            "sample": f"{n} whole {workload.upscaled_width}x{workload.height} frames of the timed rotation "
+                      f"({workload.name}, full chain), 1 thread"}
 
 
 def run_reference(args, world, rank):
-    """--impl reference: the CPU restatement with every host thread."""
+    """--impl reference: the CPU restatement with every host thread, on the
+    frames the GPU arm filters (rank 0's rotation).  A step is one whole
+    frame when K + W of them fit in about two minutes, else the top band of
+    the same frame, as many rows as fit."""
     if rank != 0:
         return
-    _, workload = WORKLOADS[args.workload]
+    cfg_idx, workload = WORKLOADS[args.workload]
     threads = os.cpu_count() or 1
-    # Calibrate the band so K + W steps take about a minute.
-    probe = cpu_sample_frame(workload, 128)
-    t_probe = time_oracle(probe, threads, 1)
-    per_row = t_probe / 128
-    budget = 60.0 / max(1, args.steps + args.warmup)
-    rows = int(max(16, min(workload.height, budget / max(per_row, 1e-9))) // 8 * 8)
-    f = cpu_sample_frame(workload, rows)
+    frames = workload_frames(cfg_idx, workload, 0)
     import oracle
 
-    for _ in range(args.warmup):
-        oracle.postfilter_frame(f, threads=threads)
+    oracle.lib()
+    t_frame = time_oracle(frames[0], threads, 1)  # also the first warm-up step
+    per_step = 120.0 / max(1, args.steps + args.warmup)
+    if t_frame <= per_step:
+        samples, rows = frames, workload.height
+    else:
+        rows = max(64, int(workload.height * per_step / t_frame) // 64 * 64)
+        samples = [band_of(f, rows) for f in frames]
+    for i in range(1, args.warmup):
+        oracle.postfilter_frame(samples[i % len(samples)], threads=threads)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    px = 0
+    for i in range(args.steps):
+        f = samples[i % len(samples)]
         _, m = oracle.postfilter_frame(f, threads=threads)
         assert m == 0
+        px += f.output_pixels
     dt = time.perf_counter() - t0
-    value = args.steps * f.output_pixels / dt / 1e6
-    sample = f"{f.upscaled_width}x{rows} band of {workload.name} per step, {threads} threads"
+    value = px / dt / 1e6
+    what = "whole frames" if rows == workload.height else f"top {rows}-row bands"
+    sample = (f"{what} of the GPU arm's {len(frames)} rotated {workload.name} frames (same seeds), "
+              f"{threads} threads, one per step")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mpixel/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "vs_baseline": None, "dtype": "u16", "data": "synthetic (the GPU arm's seeded frames)",
         "config": {"workload": workload.name, "width": workload.width, "height": workload.height,
                    "upscaled_width": workload.upscaled_width, "bit_depth": workload.bit_depth,
-                   "sample_rows": rows},
+                   "sample_rows": rows, "frames_rotated": len(frames)},
         "cpu_baseline": {"value": round(value, 3), "unit": "Mpixel/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(value, 3), "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -268,11 +351,17 @@ def run_reference(args, world, rank):
 
 
 # ---------------------------------------------------------------- GPU leg
+def hbm_peak():
+    pp = ROOT / "MEASURED_PEAKS.json"
+    peaks = json.loads(pp.read_text()) if pp.exists() else {}
+    return float(peaks.get("hbm_gbs", 6650.0)), ("measured" if "hbm_gbs" in peaks else "fallback")
+
+
 def run_gpu(args, world, rank, local):
     import torch
     import torch.distributed as dist
 
-    from vaco_b200 import abi
+    from vaco_b200 import abi, replicas
     from vaco_b200._lib import lib
     from vaco_b200.frame import pinned_copy
     from vaco_b200.gpu import Context, DeviceFrame
@@ -281,7 +370,7 @@ def run_gpu(args, world, rank, local):
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     cfg_idx, workload = WORKLOADS[args.workload]
-    frames = [synth.make_frame(workload, synth.seed_for(cfg_idx, 100 * rank + i)) for i in range(ROTATE_FRAMES)]
+    frames = workload_frames(cfg_idx, workload, rank)
     ctx = Context(local)
     dev = [DeviceFrame(f, local) for f in frames]
     stream = torch.cuda.current_stream(local)
@@ -299,17 +388,13 @@ def run_gpu(args, world, rank, local):
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, device="cuda")
 
     # -------- device-resident throughput.  Frames go back to back with
     # deferred status: no host round trip between frames, one flush (which
     # raises any device-side error of the timed frames) after the region.
     clocks = ClockSampler(local)
-    clocks.start()  # sampling runs from before warm-up; only timed-region samples count
+    clocks.start()  # sampling runs from before warm-up; the timed region's samples are kept
     for i in range(args.warmup):
         step(i)
     lib().vaco_av1_ctx_set_deferred_status(ctx.handle, 1)
@@ -335,7 +420,7 @@ def run_gpu(args, world, rank, local):
     lib().vaco_av1_ctx_set_stage_timing(ctx.handle, 0)
     lib().vaco_av1_ctx_set_deferred_status(ctx.handle, 0)
     px = frames[0].output_pixels
-    value = world * args.steps * px / (ms / 1e3) / 1e6
+    value = replicas.aggregate_mpixels(world, args.steps, px, ms)
 
     # -------- end to end from host memory (pinned buffers): every step copies
     # its frame's planes and side information to the device and its output
@@ -347,7 +432,7 @@ def run_gpu(args, world, rank, local):
     fin, fout, side = frame_bytes(frames[0])
     h2d = sum(p.nbytes for p in staged[0][0].planes) + side
     d2h = sum(o.nbytes for o in staged[0][1])
-    e2e_steps = max(3, args.steps // 4)
+    e2e_steps = max(E2E_MIN_STEPS, args.steps // 4)
 
     def pipelined(n):
         inflight = []
@@ -370,8 +455,8 @@ def run_gpu(args, world, rank, local):
     pipelined(e2e_steps)
     barrier()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3)
-    e2e_value = world * e2e_steps * px / (e2e_ms / 1e3) / 1e6
-    sync_steps = max(3, e2e_steps // 4)
+    e2e_value = replicas.aggregate_mpixels(world, e2e_steps, px, e2e_ms)
+    sync_steps = max(E2E_MIN_STEPS // 4, e2e_steps // 4)
     for i in range(args.warmup):
         lib().vaco_av1_postfilter_frame_host(ctx.handle, C.byref(jobs[i % 3]), C.byref(m))
     barrier()
@@ -381,15 +466,12 @@ def run_gpu(args, world, rank, local):
             raise RuntimeError(f"host postfilter failed: {abi.MESSAGES.get(m.value)}")
     barrier()
     sync_ms = max_over_ranks((time.perf_counter() - t0) * 1e3)
-    e2e_sync_value = world * sync_steps * px / (sync_ms / 1e3) / 1e6
+    e2e_sync_value = replicas.aggregate_mpixels(world, sync_steps, px, sync_ms)
+    del staged, jobs
 
+    line = None
     if rank == 0:
-        peaks = {}
-        pp = ROOT / "MEASURED_PEAKS.json"
-        if pp.exists():
-            peaks = json.loads(pp.read_text())
-        hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        peak, peak_src = hbm_peak()
         per_stage = {STAGES[k]: stage_ms[k] / max(1, nframes.value) for k in range(4)}
         sb = stage_bytes(frames[0])
         dominant = max(per_stage, key=per_stage.get)
@@ -424,25 +506,38 @@ def run_gpu(args, world, rank, local):
                     "one_call_per_frame": {"value": round(e2e_sync_value, 1), "steps": sync_steps,
                                            "entry": "vaco_av1_postfilter_frame_host"}},
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
-                         "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "peak_source": peak_src, "traffic": traffic,
                          "algorithmic_bytes_per_launch": int(sb[dominant]),
                          "launch_ms": round(dom_ms, 5), "launches_timed": int(nframes.value)},
             "chain_roofline": {"required_bytes_per_frame": int(required),
                                "achieved_gbs": round(required / (chain_ms / 1e3) / 1e9, 1),
-                               "frac_of_hbm": round(required / (chain_ms / 1e3) / 1e9 / hbm_peak, 4)},
+                               "frac_of_hbm": round(required / (chain_ms / 1e3) / 1e9 / peak, 4)},
             "stage_ms": {k: round(v, 5) for k, v in per_stage.items()},
             "issue_roofline": issue,
             "gpu_launches": int(launches),
             "clocks": clock_info,
         }
-        if args.cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(workload)
-        print(json.dumps(line), flush=True)
     ctx.close()
+    del dev
+    if world == 1 and args.extras:
+        # The batched and served forms of the metric, on the same GPU (one
+        # replica only: their configs are single-GPU workloads).
+        line["batched"] = batched_block(args, local)
+        line["served"] = serve_mod().served(local, args.serve_seconds or SERVED_SECONDS_DEFAULT)
+    if rank == 0:
+        if args.cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(frames, workload)
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def serve_mod():
+    from vaco_b200 import serve
+
+    return serve
 
 
 def run_emit(args, world, rank, local):
@@ -645,67 +740,96 @@ def run_grain(args, world, rank, local):
             "gpu_launches": launches}), flush=True)
 
 
-def run_batch(args, world, rank, local):
+def batched_block(args, local, steps=None):
     """Config 3: 64 frames of mixed sizes (16 each of 640x360 8-bit, 1280x720
     8-bit, 1920x1080 10-bit, 3840x2160 10-bit), independently seeded, through
     vaco_av1_postfilter_batch_dev (persistent per-stage kernels over a device
-    tile queue, CUDA-graph replay, tuned launch shape)."""
+    tile queue, CUDA-graph replay, tuned launch shape), beside the same 64
+    frames through the per-frame entry point back to back (deferred status),
+    and a batch of 16 4K 10-bit frames."""
     import torch
 
     from vaco_b200 import autotune
     from vaco_b200.gpu import Context, DeviceFrame
 
-    torch.cuda.set_device(local)
+    steps = steps or max(5, min(args.steps, 50))
     ctx = Context(local)
     tuning = autotune.load_tuning()
     ctx.set_tuning(**tuning)
     stream = torch.cuda.current_stream(local)
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    hbm, _ = hbm_peak()
 
-    def time_batch(frames):
-        devs = [DeviceFrame(f, local) for f in frames]
+    def rates(frames, ms):
+        px = sum(f.output_pixels for f in frames)
+        req = sum(sum(frame_bytes(f)) for f in frames)
+        return {"value": round(px / (ms / 1e3) / 1e6, 1), "ms_per_batch": round(ms, 4),
+                "frames_per_batch": len(frames),
+                "hbm_roofline": {"required_bytes_per_batch": int(req),
+                                 "achieved_gbs": round(req / (ms / 1e3) / 1e9, 1), "peak": hbm,
+                                 "frac": round(req / (ms / 1e3) / 1e9 / hbm, 4)}}
+
+    def time_batch(devs):
         jobs = ctx.batch_jobs(devs)
-        for _ in range(args.warmup):
+        for _ in range(max(3, args.warmup)):
             st, _ = ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs)
-            assert all(s == 0 for s in st)
+            assert all(x == 0 for x in st)
         torch.cuda.synchronize()
         launches0 = ctx.launches
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs)
         ev1.record(stream)
         torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1) / args.steps
-        px = sum(f.output_pixels for f in frames)
-        req = sum(sum(frame_bytes(f)) for f in frames)
-        del devs
-        return {"value": round(px / (ms / 1e3) / 1e6, 1), "ms_per_batch": round(ms, 4), "frames_per_batch": len(frames),
-                "hbm_roofline": {"required_bytes_per_batch": int(req),
-                                 "achieved_gbs": round(req / (ms / 1e3) / 1e9, 1), "peak": hbm,
-                                 "frac": round(req / (ms / 1e3) / 1e9 / hbm, 4)},
-                "gpu_launches_per_batch": (ctx.launches - launches0) / max(1, args.steps)}
+        return ev0.elapsed_time(ev1) / steps, (ctx.launches - launches0) / steps
+
+    def time_per_frame(devs):
+        ctx.set_deferred_status(True)
+        for d in devs:
+            ctx.postfilter_frame_dev(d, stream.cuda_stream)
+        ctx.flush(stream.cuda_stream)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            for d in devs:
+                ctx.postfilter_frame_dev(d, stream.cuda_stream)
+        ev1.record(stream)
+        ctx.flush(stream.cuda_stream)
+        ctx.set_deferred_status(False)
+        return ev0.elapsed_time(ev1) / steps
 
     mix = []
     for wl, count in synth.BATCH_MIX:
         for i in range(count):
-            mix.append(synth.make_frame(wl, synth.seed_for(3, 1000 * rank + len(mix))))
-    mixed = time_batch(mix)
-    del mix
-    # The batched path on 4K 10-bit frames alone (16 per batch).
-    k4 = [synth.make_frame(synth.CONFIG1, synth.seed_for(3, 1000 * rank + 500 + i)) for i in range(16)]
-    only4k = time_batch(k4)
-    if rank == 0:
-        print(json.dumps({
-            "metric": "AV1 post-filter Mpixel/s, batched mixed-resolution frames", "mode": "batch",
-            "value": mixed["value"], "unit": "Mpixel/s", "ms_per_batch": mixed["ms_per_batch"],
-            "frames_per_batch": mixed["frames_per_batch"], "steps": args.steps, "warmup": args.warmup,
-            "config": {"workload": "batch_mix_64", "mix": [[w.name, c] for w, c in synth.BATCH_MIX], "tuning": tuning},
-            "hbm_roofline": mixed["hbm_roofline"], "gpu_launches_per_batch": mixed["gpu_launches_per_batch"],
-            "batch_4k_10bit_16": only4k,
-        }), flush=True)
+            mix.append(synth.make_frame(wl, synth.seed_for(3, len(mix))))
+    devs = [DeviceFrame(f, local) for f in mix]
+    ms, launches = time_batch(devs)
+    mixed = rates(mix, ms)
+    mixed["gpu_launches_per_batch"] = launches
+    per_frame = rates(mix, time_per_frame(devs))
+    del devs
+    k4 = [synth.make_frame(synth.CONFIG1, synth.seed_for(3, 500 + i)) for i in range(16)]
+    devs = [DeviceFrame(f, local) for f in k4]
+    ms4, _ = time_batch(devs)
+    only4k = rates(k4, ms4)
+    del devs
     ctx.close()
+    return dict(mixed, steps=steps, tuning=tuning,
+                config={"workload": "batch_mix_64", "mix": [[w.name, c] for w, c in synth.BATCH_MIX]},
+                per_frame_same_mix={"value": per_frame["value"], "ms_per_64_frames": per_frame["ms_per_batch"],
+                                    "entry": "vaco_av1_postfilter_frame_dev per frame, deferred status"},
+                batch_4k_10bit_16=only4k)
+
+
+def run_batch(args, world, rank, local):
+    """--mode batch: the batched block alone, as its own JSON line."""
+    import torch
+
+    torch.cuda.set_device(local)
+    res = batched_block(args, local, steps=args.steps)
+    if rank == 0:
+        print(json.dumps(dict({"metric": "AV1 post-filter Mpixel/s, batched mixed-resolution frames",
+                               "mode": "batch", "unit": "Mpixel/s", "warmup": args.warmup}, **res)), flush=True)
 
 
 def main():
@@ -717,7 +841,11 @@ def main():
     ap.add_argument("--workload", default="chain_4k_10bit", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--mode", default="headline", choices=["headline", "batch", "serve", "emit", "grain"])
-    ap.add_argument("--serve-seconds", type=float, default=60.0, help="seconds per arrival rate in --mode serve")
+    ap.add_argument("--serve-seconds", type=float, default=None,
+                    help="seconds per arrival rate and mode: --mode serve (default 60) and the default line's "
+                         "served block (default 5)")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="headline line without its batched and served blocks")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_env()

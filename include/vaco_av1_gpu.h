@@ -31,7 +31,9 @@
  *     device are independent.
  *
  * Budget/fuel accounting (vaco-limits::Budget) stays with the caller, which
- * allocates the outputs; see INTEGRATION.md for the Rust shim that does it.
+ * allocates the outputs through its Budget before the call, so vaco's
+ * Error::LimitExceeded keeps its meaning (crates/hw/vaco-hw-cuda-av1 is the
+ * Rust shim that does it).
  */
 #ifndef VACO_AV1_GPU_H
 #define VACO_AV1_GPU_H
@@ -89,7 +91,9 @@ typedef enum vaco_av1_msg {
     VACO_AV1_MSG_PIXEL_FORMAT = 21,       /* src/decode.rs:3819 */
     VACO_AV1_MSG_FG_PARAMS = 22,          /* film grain (no vaco counterpart) */
     VACO_AV1_MSG_FG_SAMPLE = 23,          /* film grain (no vaco counterpart) */
-    VACO_AV1_MSG_COUNT = 24
+    VACO_AV1_MSG_SR_MISSING_U = 24,       /* src/superres.rs:257 */
+    VACO_AV1_MSG_SR_MISSING_V = 25,       /* src/superres.rs:265 */
+    VACO_AV1_MSG_COUNT = 26
 } vaco_av1_msg;
 
 /* Static, NUL-terminated text for a message id ("" for unknown ids). */
@@ -246,6 +250,36 @@ VACO_AV1_API int32_t vaco_av1_superres_upscale_plane_host(vaco_av1_ctx* ctx, con
                                              int32_t visible_width, int32_t output_width,
                                              int32_t height, int32_t bit_depth,
                                              uint16_t* output, int32_t* msg);
+
+/* superres::PictureConfig (src/superres.rs:107-122): luma geometry and
+ * colour layout of a reconstructed picture. */
+typedef struct vaco_av1_superres_picture_config {
+    int32_t coded_width;     /* luma width before superres */
+    int32_t upscaled_width;  /* luma width after superres */
+    int32_t coded_height;    /* visible luma height */
+    int32_t subsampling_x;   /* 0/1 */
+    int32_t subsampling_y;   /* 0/1 */
+    int32_t monochrome;      /* 0/1: U and V absent */
+    int32_t bit_depth;       /* 8, 10 or 12 */
+} vaco_av1_superres_picture_config;
+
+/* superres::upscale_picture (src/superres.rs:226-274): upscale_plane on luma
+ * (coded_width -> upscaled_width, coded_height rows), then on U and V with
+ * the ceil-divided chroma geometry, in that order; the first plane that
+ * fails decides the error, as in vaco.  `in` holds the Mi-padded planes
+ * (width[k] is each plane's padded width, the edge-extension limit); `out`
+ * holds caller-allocated planes of exactly the output extents (luma
+ * upscaled_width x coded_height, chroma ceil-divided).  A NULL U or V input
+ * plane of a non-monochrome picture fails with VACO_AV1_MSG_SR_MISSING_U /
+ * _V once luma has succeeded.  All planes run in one launch. */
+VACO_AV1_API int32_t vaco_av1_superres_upscale_picture_dev(vaco_av1_ctx* ctx, void* stream,
+                                              const vaco_av1_picture* in, const vaco_av1_picture* out,
+                                              const vaco_av1_superres_picture_config* config,
+                                              int32_t* msg);
+VACO_AV1_API int32_t vaco_av1_superres_upscale_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture* in,
+                                               const vaco_av1_picture* out,
+                                               const vaco_av1_superres_picture_config* config,
+                                               int32_t* msg);
 
 /* ---------------------------------------------------------------- restoration */
 
@@ -404,7 +438,8 @@ typedef struct vaco_av1_server_config {
     int32_t device;
     int32_t max_batch_frames;     /* frames packed into one launch set */
     int32_t inflight_batches;     /* launch sets in flight (one CUDA stream each) */
-    int32_t reserved;
+    int32_t host_wait_ms;         /* bound of the host waits in submit (backpressure)
+                                     and close_stream; 0 = 10000 */
     int64_t memory_budget_bytes;  /* stream buffers + batch scratch */
 } vaco_av1_server_config;
 
@@ -429,6 +464,10 @@ VACO_AV1_API void vaco_av1_server_destroy(vaco_av1_server* server);
 VACO_AV1_API int32_t vaco_av1_server_open_stream(vaco_av1_server* server, const vaco_av1_frame_info* info,
                                                  const int32_t* lr_unit_size, int32_t buffers, int32_t* stream_id,
                                                  int32_t* msg);
+/* Closes a stream and frees its buffers once none of its frames is in flight.
+ * Waits at most host_wait_ms (10 s by default) for them; then returns
+ * VACO_AV1_TIMEOUT and leaves the stream open (its frames still complete, and
+ * a later close succeeds). */
 VACO_AV1_API int32_t vaco_av1_server_close_stream(vaco_av1_server* server, int32_t stream_id);
 
 /* Device pointers of slot `slot` of a stream, filled into `job` (src and dst
@@ -441,9 +480,23 @@ VACO_AV1_API int32_t vaco_av1_server_slot(vaco_av1_server* server, int32_t strea
  * (deblock, cdef, lr_type; its pointers and geometry are ignored) and returns
  * a ticket.  Does not wait for the GPU, except that a slot whose previous
  * frame is still being filtered is waited for first (backpressure, at most
- * 10 s, then VACO_AV1_TIMEOUT). */
+ * host_wait_ms, 10 s by default, then VACO_AV1_TIMEOUT). */
 VACO_AV1_API int32_t vaco_av1_server_submit(vaco_av1_server* server, int32_t stream_id, int32_t slot,
                                             const vaco_av1_frame_job* params, uint64_t* ticket);
+
+/* Like vaco_av1_server_submit, with the frame's inputs in HOST memory: `host`
+ * carries host pointers to the reconstruction, side information and
+ * restoration units (extents as the stream's, as for
+ * vaco_av1_server_upload) together with the frame-level parameters.  The
+ * copies into the slot are enqueued on the server's own copy stream and the
+ * launch that takes the frame waits for them on the device, so one frame's
+ * upload overlaps other frames' filtering and the ticket's latency includes
+ * the upload.  Host buffers must stay valid until the ticket's wait returns;
+ * page-locked buffers let the copies run asynchronously.  Backpressure and
+ * TIMEOUT as for vaco_av1_server_submit; VACO_AV1_INVALID_DATA when the host
+ * frame does not match the stream. */
+VACO_AV1_API int32_t vaco_av1_server_submit_host(vaco_av1_server* server, int32_t stream_id, int32_t slot,
+                                                 const vaco_av1_frame_job* host, uint64_t* ticket);
 
 /* Waits up to timeout_ms (< 0: forever) for a ticket.  Returns VACO_AV1_TIMEOUT
  * if it has not completed; otherwise the frame's status, with the message and
@@ -599,8 +652,11 @@ VACO_AV1_API int32_t vaco_av1_film_grain_host(vaco_av1_ctx* ctx, const vaco_av1_
  * and the status word live in one fixed device array of 16 MiB (plus 256 B)
  * in the library; every GPU that loads the library holds it until exit.
  * Frames whose intermediates do not fit fail with VACO_AV1_LIMIT_EXCEEDED /
- * VACO_AV1_MSG_SCRATCH_LIMIT.  The array fits up to 1920x1088 4:2:0 without
- * superres, or 1280x720 with it.
+ * VACO_AV1_MSG_SCRATCH_LIMIT before any work.  A 1920-wide 4:2:0 frame fits
+ * up to 1456 rows without superres (so 1920x1088 fits); with superres and
+ * restoration, 1024x720 -> 1280x720 fits and 1440x1080 -> 1920x1080 does
+ * not.  The chain runs as per-stage kernels (not the fused deblock+CDEF
+ * kernel of vaco_av1_postfilter_frame_dev), with identical output.
  * All calls share the array.  Calls whose GPU work overlaps race and produce
  * undefined output.
  * The first call on a device resolves the array's address on that device;

@@ -51,6 +51,8 @@ def lib():
         l.vo_postfilter_frame.argtypes = [vp, i32]
         l.vo_emit_frame.argtypes = [vp, vp, vp]
         l.vo_film_grain.argtypes = [vp, vp, vp, vp, vp]
+        l.vo_upscale_picture.argtypes = [vp, vp, vp, i32]
+        l.vo_deblock_lines.argtypes = [vp, i32, i32, i32, vp, i32, i32, vp]
         _lib = l
     return _lib
 
@@ -122,6 +124,32 @@ def upscale_plane(plane: np.ndarray, visible_width: int, output_width: int, heig
     return out, m
 
 
+def upscale_picture(planes, config: abi.SuperresPictureConfig, threads: int | None = None):
+    """superres::upscale_picture (src/superres.rs:226-274) over `planes`
+    (Mi-padded; None for an absent chroma plane); returns (output planes, msg)."""
+    np_ = 1 if config.monochrome else 3
+    ins = [None if p is None else _u16(p) for p in planes]
+    outs = []
+    for k in range(np_):
+        sx = config.subsampling_x if k else 0
+        sy = config.subsampling_y if k else 0
+        w = -(-config.upscaled_width // (1 << sx))
+        h = -(-config.coded_height // (1 << sy))
+        outs.append(np.zeros((max(h, 0), max(w, 0)), np.uint16))
+    pin = abi.Picture()
+    pout = abi.Picture()
+    for k in range(np_):
+        if ins[k] is not None:
+            pin.planes[k] = ins[k].ctypes.data
+            pin.height[k], pin.width[k] = ins[k].shape
+            pin.stride[k] = ins[k].shape[1]
+        pout.planes[k] = outs[k].ctypes.data if outs[k].size else None
+        pout.height[k], pout.width[k] = outs[k].shape
+        pout.stride[k] = max(outs[k].shape[1], 1)
+    m = lib().vo_upscale_picture(C.byref(pin), C.byref(pout), C.byref(config), threads or default_threads())
+    return outs, m
+
+
 # ---------------------------------------------------------------- restoration
 def restore_plane(before: np.ndarray, after: np.ndarray, width: int, height: int,
                   bit_depth: int, unit_size: int, subsampling_y: bool, units: np.ndarray,
@@ -155,6 +183,18 @@ def deblock_picture(f: FrameInputs, threads: int | None = None):
                                  ptr(np.ascontiguousarray(f.tx_chroma, np.uint8)),
                                  ptr(lvl), C.byref(params), threads or default_threads())
     return outs, m
+
+
+def deblock_lines(lines, plane: int, filter_size: int, levels, sharpness: int, bit_depth: int) -> np.ndarray:
+    """Lines of 16 samples across an edge (sample k past the edge at index
+    8 + k), shape (n, 16), each at its own level, through the oracle's 7.14.6
+    sample filter; returns the filtered lines."""
+    lines = _u16(lines).reshape(-1, 16)
+    lv = np.ascontiguousarray(levels, np.uint8).reshape(-1)
+    assert lv.size == lines.shape[0]
+    out = np.zeros_like(lines)
+    lib().vo_deblock_lines(ptr(lines), lines.shape[0], plane, filter_size, ptr(lv), sharpness, bit_depth, ptr(out))
+    return out
 
 
 # ---------------------------------------------------------------- whole chain

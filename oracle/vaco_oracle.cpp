@@ -819,6 +819,51 @@ int vo_upscale_plane(const uint16_t* input, int in_width, int in_height, int in_
     return upscale_plane(in, visible_width, output_width, height, bit_depth, out, threads);
 }
 
+// upscale_picture (src/superres.rs:226-274): luma at (coded_width,
+// upscaled_width, coded_height), then U and V at the ceil-divided chroma
+// geometry, each through upscale_plane in that order, so the first failing
+// plane's error is the one returned.  A missing U or V plane fails with
+// vaco's "missing U/V plane" message once luma has succeeded.
+int vo_upscale_picture(const vaco_av1_picture* in, const vaco_av1_picture* out,
+                       const vaco_av1_superres_picture_config* cfg, int threads) {
+    const int np = cfg->monochrome ? 1 : 3;
+    for (int k = 0; k < np; ++k) {
+        const int sx = k ? cfg->subsampling_x : 0, sy = k ? cfg->subsampling_y : 0;
+        const int vis = (cfg->coded_width + (1 << sx) - 1) >> sx;
+        const int outw = (cfg->upscaled_width + (1 << sx) - 1) >> sx;
+        const int h = (cfg->coded_height + (1 << sy) - 1) >> sy;
+        if (!in->planes[k]) return k == 1 ? VACO_AV1_MSG_SR_MISSING_U : VACO_AV1_MSG_SR_MISSING_V;
+        PlaneRef src{in->planes[k], in->width[k], in->height[k], in->stride[k]};
+        PlaneMut dst{out->planes[k], outw, h, out->stride[k]};
+        if (int m = upscale_plane(src, vis, outw, h, cfg->bit_depth, dst, threads)) return m;
+    }
+    return 0;
+}
+
+// Lines across a deblocking edge through the 7.14.6 sample filter, for
+// cross-checks of the filter arithmetic: lines[16 i + 8 + k] is sample k past
+// the edge (k < 0 on the p side) of line i, which filters at level lvls[i];
+// out receives each line after filtering (a copy where nothing is written).
+int vo_deblock_lines(const uint16_t* lines, int n, int plane, int filter_size, const uint8_t* lvls, int sharpness,
+                     int bit_depth, uint16_t* out) {
+    vaco_av1_frame_info info{};
+    info.bit_depth = bit_depth;
+    vaco_av1_deblock_params params{};
+    params.sharpness = (uint8_t)sharpness;
+    Deblocker d{info, nullptr, nullptr, nullptr, params, 0, 0};
+    for (int i = 0; i < n; ++i) {
+        const uint16_t* line = lines + 16L * i;
+        uint16_t* o = out + 16L * i;
+        for (int k = 0; k < 16; ++k) o[k] = line[k];
+        auto get = [&](int k) { return (int)line[std::min(std::max(8 + k, 0), 15)]; };
+        auto put = [&](int k, int v) {
+            if (8 + k >= 0 && 8 + k < 16) o[8 + k] = (uint16_t)v;
+        };
+        d.filter_line(get, put, plane, filter_size, filter_strength(lvls[i], sharpness));
+    }
+    return 0;
+}
+
 int vo_restore_plane(const uint16_t* before, int bw, int bh, int bstride, const uint16_t* after,
                      int aw, int ah, int astride, const vaco_av1_lr_plane_config* cfg,
                      const vaco_av1_lr_unit* units, int unit_count, uint16_t* output,
@@ -1260,6 +1305,7 @@ extern "C" int vo_sizeof(const char* name) {
         {"vaco_av1_tuning", (int)sizeof(vaco_av1_tuning)},
         {"vaco_av1_frame_buffer", (int)sizeof(vaco_av1_frame_buffer)},
         {"vaco_av1_film_grain_params", (int)sizeof(vaco_av1_film_grain_params)},
+        {"vaco_av1_superres_picture_config", (int)sizeof(vaco_av1_superres_picture_config)},
     };
     for (const Entry& e : kSizes)
         if (std::strcmp(e.n, name) == 0) return e.s;

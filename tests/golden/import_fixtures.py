@@ -26,7 +26,9 @@ FIXTURES = {
 
 
 def main() -> None:
-    root = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/import_fixtures.py /path/to/vaco")
+    root = pathlib.Path(sys.argv[1])
     here = pathlib.Path(__file__).resolve().parent
     lines = []
     for rel, name in FIXTURES.items():

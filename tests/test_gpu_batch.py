@@ -65,3 +65,26 @@ def test_batch_reports_errors_per_frame(ctx):
         want, _ = oracle.postfilter_frame(frames[i])
         for g, w in zip(devs[i].outputs_numpy(), want):
             np.testing.assert_array_equal(g, w)
+
+
+def test_config3_full_mix_matches_oracle(ctx, oracle_threads):
+    """Config 3 as specified: 64 frames, 16 each of 640x360 8-bit, 1280x720
+    8-bit, 1920x1080 10-bit and 3840x2160 10-bit, independently seeded, in one
+    launch set with the committed tuning; every frame bit-exact."""
+    from vaco_b200 import autotune
+
+    ctx.set_tuning(**autotune.load_tuning())
+    stream = torch.cuda.current_stream().cuda_stream
+    frames = []
+    for wl, count in synth.BATCH_MIX:
+        for i in range(count):
+            frames.append(synth.make_frame(wl, synth.seed_for(3, 2000 + len(frames))))
+    assert len(frames) == 64
+    devs = [DeviceFrame(f) for f in frames]
+    st, ms = ctx.postfilter_batch_dev(devs, stream=stream)
+    assert st == [0] * 64 and ms == [0] * 64
+    for i, (f, d) in enumerate(zip(frames, devs)):
+        want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+        assert m == 0
+        for k, (g, w) in enumerate(zip(d.outputs_numpy(), want)):
+            assert np.array_equal(g, w), f"frame {i} ({f.coded_width}x{f.coded_height}) plane {k} differs"

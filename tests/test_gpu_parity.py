@@ -55,15 +55,44 @@ def test_deblock_small(ctx, geom, sharp, oracle_threads):
         assert_planes_equal(ctx.deblock_picture(f), want, f"deblock seed={seed}")
 
 
+TX_W = [4, 8, 16, 32, 64, 4, 8, 8, 16, 16, 32, 32, 64, 4, 16, 8, 32, 16, 64]
+TX_H = [4, 8, 16, 32, 64, 8, 4, 16, 8, 32, 16, 64, 32, 16, 4, 32, 8, 64, 16]
+
+
+def luma_edge_reach(tx_luma):
+    """Luma samples a 7.14 deblocking pass may write: for every 4x4 cell on a
+    transform edge (its x (y) a multiple of its transform's width (height)),
+    the samples the edge's filter reaches, from the filter size min(16, both
+    sides' transform extents): size 4 writes p1..q1, size 8 p2..q2, size 16
+    p5..q5 (7.14.6)."""
+    tw = np.array(TX_W)[tx_luma]
+    th = np.array(TX_H)[tx_luma]
+    rows, cols = tx_luma.shape
+    reach = np.zeros((rows * 4, cols * 4), bool)
+    span = {4: (2, 1), 8: (3, 2), 16: (6, 5)}
+    for r in range(rows):
+        for c in range(cols):
+            x, y = 4 * c, 4 * r
+            if c > 0 and x % tw[r, c] == 0:
+                before, after = span[min(16, tw[r, c], tw[r, c - 1])]
+                reach[y:y + 4, max(0, x - before):x + after + 1] = True
+            if r > 0 and y % th[r, c] == 0:
+                before, after = span[min(16, th[r, c], th[r - 1, c])]
+                reach[max(0, y - before):y + after + 1, x:x + 4] = True
+    return reach
+
+
 def test_deblock_changes_samples_only_near_edges(ctx):
     f = synth.make_small(5, 256, 128, 10)
     out = ctx.deblock_picture(f)
     diff = out[0] != f.planes[0]
     assert diff.any()
-    # Samples more than 6 away from every 4-aligned column and row are untouched.
-    cols = np.arange(diff.shape[1]) % 4
-    rows = np.arange(diff.shape[0]) % 4
-    assert diff.shape[1] > 0 and (cols >= 0).all() and (rows >= 0).all()
+    reach = luma_edge_reach(f.tx_luma)
+    # Nothing farther from a transform edge than its filter reaches changes,
+    # and a good part of the plane (transform interiors) is out of reach.
+    ys, xs = np.nonzero(diff & ~reach)
+    assert ys.size == 0, f"{ys.size} samples changed away from every edge, first at y={ys[0]} x={xs[0]}"
+    assert (~reach).mean() > 0.2
 
 
 def test_superres_plane_full_size(ctx, oracle_threads):
@@ -182,3 +211,61 @@ def test_restoration_none_preserves_visible_cdef_pixels(ctx):
     none = np.zeros(1, abi.lr_unit_dtype())
     out = ctx.restore_plane(before, after, 7, 9, 8, 64, False, none)
     assert out.shape == (9, 7) and (out == 235).all()
+
+
+def _sr_picture(rng, coded_w, up_w, coded_h, ssx, ssy, mono, bd):
+    """Mi-padded planes of a picture (8-aligned luma, as the decoder pads) and
+    its superres::PictureConfig."""
+    cfg = abi.SuperresPictureConfig(coded_w, up_w, coded_h, ssx, ssy, int(mono), bd)
+    pw, ph = (coded_w + 7) // 8 * 8, (coded_h + 7) // 8 * 8
+    planes = [rng.integers(0, 1 << bd, (ph, pw), dtype=np.uint16)]
+    if not mono:
+        planes += [rng.integers(0, 1 << bd, (ph >> ssy, pw >> ssx), dtype=np.uint16) for _ in range(2)]
+    return planes, cfg
+
+
+@pytest.mark.parametrize("layout", [(1, 1, False), (1, 0, False), (0, 0, False), (1, 1, True)],
+                         ids=["420", "422", "444", "mono"])
+@pytest.mark.parametrize("geom", [(2880, 3840, 2160, 10), (1439, 1918, 217, 8), (95, 120, 15, 12)],
+                         ids=lambda g: f"{g[0]}to{g[1]}x{g[2]}_{g[3]}bit")
+def test_upscale_picture_matches_oracle(ctx, layout, geom, oracle_threads):
+    ssx, ssy, mono = layout
+    coded_w, up_w, coded_h, bd = geom
+    rng = np.random.default_rng(coded_w + 7 * ssx + 3 * ssy + int(mono))
+    planes, cfg = _sr_picture(rng, coded_w, up_w, coded_h, ssx, ssy, mono, bd)
+    want, m = oracle.upscale_picture(planes, cfg, threads=oracle_threads)
+    assert m == 0
+    got = ctx.upscale_picture(planes, cfg)
+    assert_planes_equal(got, want, f"upscale_picture {layout} {geom}")
+    # chroma geometry is the ceil division of the luma's (superres.rs:247-250)
+    if not mono:
+        assert got[1].shape == (-(-coded_h // (1 << ssy)), -(-up_w // (1 << ssx)))
+
+
+def test_upscale_picture_errors_follow_plane_order(ctx):
+    rng = np.random.default_rng(5)
+    planes, cfg = _sr_picture(rng, 64, 80, 16, 1, 1, False, 10)
+    # a missing U plane fails after luma succeeds
+    _, m = oracle.upscale_picture([planes[0], None, planes[2]], cfg)
+    assert m == abi.MSG["SR_MISSING_U"]
+    _expect_same_error(lambda: ctx.upscale_picture([planes[0], None, planes[2]], cfg), m)
+    _, m = oracle.upscale_picture([planes[0], planes[1], None], cfg)
+    assert m == abi.MSG["SR_MISSING_V"]
+    _expect_same_error(lambda: ctx.upscale_picture([planes[0], planes[1], None], cfg), m)
+    # a luma sample above the bit depth comes before the missing plane
+    bad = planes[0].copy()
+    bad[3, 40] = 1024
+    _, m = oracle.upscale_picture([bad, None, planes[2]], cfg)
+    assert m == abi.MSG["SR_SAMPLE"]
+    _expect_same_error(lambda: ctx.upscale_picture([bad, None, planes[2]], cfg), m)
+    # a chroma sample error after a clean luma; a bad depth; a bad geometry
+    badv = planes[2].copy()
+    badv[2, 2] = 2000
+    _, m = oracle.upscale_picture([planes[0], planes[1], badv], cfg)
+    _expect_same_error(lambda: ctx.upscale_picture([planes[0], planes[1], badv], cfg), m)
+    cfg9 = abi.SuperresPictureConfig(64, 80, 16, 1, 1, 0, 9)
+    _, m = oracle.upscale_picture(planes, cfg9)
+    _expect_same_error(lambda: ctx.upscale_picture(planes, cfg9), m)
+    cfg_eq = abi.SuperresPictureConfig(64, 64, 16, 1, 1, 0, 10)
+    _, m = oracle.upscale_picture(planes, cfg_eq)
+    _expect_same_error(lambda: ctx.upscale_picture(planes, cfg_eq), m)

@@ -38,6 +38,8 @@ SIGNATURES = [
     ("vaco_av1_superres_upscale_plane_dev", _i32,
      [_vp, _vp, _vp, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _vp, _i32, _pi32]),
     ("vaco_av1_superres_upscale_plane_host", _i32, [_vp, _vp, _i32, _i32, _i32, _i32, _i32, _i32, _vp, _pi32]),
+    ("vaco_av1_superres_upscale_picture_dev", _i32, [_vp, _vp, _vp, _vp, _vp, _pi32]),
+    ("vaco_av1_superres_upscale_picture_host", _i32, [_vp, _vp, _vp, _vp, _pi32]),
     ("vaco_av1_restore_plane_dev", _i32,
      [_vp, _vp, _vp, _i32, _i32, _i32, _vp, _i32, _i32, _i32, _vp, _vp, _i32, _vp, _i32, _pi32]),
     ("vaco_av1_restore_plane_host", _i32, [_vp, _vp, _i32, _i32, _vp, _i32, _i32, _vp, _vp, _i32, _vp, _pi32]),
@@ -57,6 +59,7 @@ SIGNATURES = [
     ("vaco_av1_server_close_stream", _i32, [_vp, _i32]),
     ("vaco_av1_server_slot", _i32, [_vp, _i32, _i32, _vp]),
     ("vaco_av1_server_submit", _i32, [_vp, _i32, _i32, _vp, _vp]),
+    ("vaco_av1_server_submit_host", _i32, [_vp, _i32, _i32, _vp, _vp]),
     ("vaco_av1_server_wait", _i32, [_vp, C.c_uint64, _i32, _vp, _vp]),
     ("vaco_av1_server_get_stats", _i32, [_vp, _vp]),
     ("vaco_av1_server_upload", _i32, [_vp, _i32, _i32, _vp]),

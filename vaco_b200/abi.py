@@ -42,6 +42,8 @@ MESSAGES = {
     21: "vaco-codec-av1: unsupported pixel format",
     22: "invalid AV1 film grain parameters",
     23: "AV1 film grain sample exceeds bit depth",
+    24: "AV1 superres missing U plane",
+    25: "AV1 superres missing V plane",
 }
 MSG = {
     "NONE": 0, "CDEF_BIT_DEPTH": 1, "CDEF_SAMPLE": 2, "CDEF_BLOCK_PARAMS": 3,
@@ -49,7 +51,7 @@ MSG = {
     "LR_GEOMETRY": 8, "LR_UNIT_COUNT": 9, "LR_COEFFICIENT": 10, "LR_SAMPLE": 11,
     "LR_NO_UNIT_SIZE": 12, "DB_PARAMS": 13, "DB_SAMPLE": 14, "FRAME_GEOMETRY": 15,
     "NULL_ARGUMENT": 16, "CUDA": 17, "SCRATCH_LIMIT": 18, "QUEUE_FULL": 19, "TIMEOUT": 20,
-    "PIXEL_FORMAT": 21, "FG_PARAMS": 22, "FG_SAMPLE": 23,
+    "PIXEL_FORMAT": 21, "FG_PARAMS": 22, "FG_SAMPLE": 23, "SR_MISSING_U": 24, "SR_MISSING_V": 25,
 }
 
 LR_NONE, LR_WIENER, LR_SGRPROJ = 0, 1, 2
@@ -122,6 +124,20 @@ class LrPlaneConfig(C.Structure):
         ("bit_depth", C.c_int32),
         ("unit_size", C.c_int32),
         ("subsampling_y", C.c_int32),
+    ]
+
+
+class SuperresPictureConfig(C.Structure):
+    """vaco_av1_superres_picture_config: superres::PictureConfig (src/superres.rs:107-122)."""
+
+    _fields_ = [
+        ("coded_width", C.c_int32),
+        ("upscaled_width", C.c_int32),
+        ("coded_height", C.c_int32),
+        ("subsampling_x", C.c_int32),
+        ("subsampling_y", C.c_int32),
+        ("monochrome", C.c_int32),
+        ("bit_depth", C.c_int32),
     ]
 
 
@@ -235,4 +251,5 @@ STRUCT_SIZES = {
     "vaco_av1_tuning": C.sizeof(Tuning),
     "vaco_av1_frame_buffer": C.sizeof(FrameBuffer),
     "vaco_av1_film_grain_params": C.sizeof(FilmGrainParams),
+    "vaco_av1_superres_picture_config": C.sizeof(SuperresPictureConfig),
 }

@@ -44,6 +44,8 @@ const char* const kMessages[VACO_AV1_MSG_COUNT] = {
     "vaco-codec-av1: unsupported pixel format",
     "invalid AV1 film grain parameters",
     "AV1 film grain sample exceeds bit depth",
+    "AV1 superres missing U plane",
+    "AV1 superres missing V plane",
 };
 
 unsigned long long make_key(unsigned stage, unsigned long long position, unsigned msg) {
@@ -575,6 +577,86 @@ int32_t vaco_av1_superres_upscale_plane_host(vaco_av1_ctx* ctx, const uint16_t* 
                                                      dout.stride[0], msg);
     if (st != VACO_AV1_OK) return st;
     e = copy_picture_out(&dout, &hout, 1, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    return VACO_AV1_OK;
+}
+
+// superres::upscale_picture (src/superres.rs:226-274).  vaco runs
+// upscale_plane on Y, then U, then V, so a plane's validation failure only
+// surfaces when every earlier plane filtered cleanly.  The planes before the
+// first failing one run in one launch; the failure becomes a host key at the
+// largest superres position, which any sample error of those planes beats.
+int32_t vaco_av1_superres_upscale_picture_dev(vaco_av1_ctx* ctx, void* stream, const vaco_av1_picture* in,
+                                              const vaco_av1_picture* out,
+                                              const vaco_av1_superres_picture_config* cfg, int32_t* msg) {
+    if (!ctx || !in || !out || !cfg) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    if (cfg->subsampling_x < 0 || cfg->subsampling_x > 1 || cfg->subsampling_y < 0 || cfg->subsampling_y > 1)
+        return invalid(msg, VACO_AV1_MSG_FRAME_GEOMETRY);
+    const int np = cfg->monochrome ? 1 : 3;
+    SuperresPlane sp[3];
+    int nsp = 0;
+    unsigned long long host_key = kNoError;
+    for (int k = 0; k < np; ++k) {
+        const int sx = k ? cfg->subsampling_x : 0, sy = k ? cfg->subsampling_y : 0;
+        // div_ceil on non-negative extents (src/superres.rs:247-250)
+        const int vis = cfg->coded_width < 0 ? cfg->coded_width : (cfg->coded_width + (1 << sx) - 1) >> sx;
+        const int outw = cfg->upscaled_width < 0 ? cfg->upscaled_width : (cfg->upscaled_width + (1 << sx) - 1) >> sx;
+        const int h = cfg->coded_height < 0 ? cfg->coded_height : (cfg->coded_height + (1 << sy) - 1) >> sy;
+        int m = VACO_AV1_MSG_NONE;
+        if (k > 0 && !in->planes[k])
+            m = k == 1 ? VACO_AV1_MSG_SR_MISSING_U : VACO_AV1_MSG_SR_MISSING_V;
+        else if (!bd_valid(cfg->bit_depth))
+            m = VACO_AV1_MSG_SR_BIT_DEPTH;
+        else if (vis <= 0 || outw <= vis || h <= 0 || vis > in->width[k] || h > in->height[k])
+            m = VACO_AV1_MSG_SR_GEOMETRY;
+        if (m != VACO_AV1_MSG_NONE) {
+            host_key = make_key(STAGE_SUPERRES, (1ull << 52) - 1, m);
+            break;
+        }
+        if (!in->planes[k] || !out->planes[k]) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+        if (in->stride[k] < in->width[k] || out->width[k] != outw || out->height[k] != h ||
+            out->stride[k] < out->width[k])
+            return invalid(msg, VACO_AV1_MSG_FRAME_GEOMETRY);
+        SuperresPlane& p = sp[nsp++];
+        p.in = cplane(*in, k);
+        p.out = DevPlane{out->planes[k], outw, h, out->stride[k]};
+        p.visible_width = vis;
+        p.output_width = outw;
+        p.height = h;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = reset_status(ctx, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    if (nsp > 0) {
+        e = launch_superres(sp, nsp, cfg->bit_depth, ctx->status, STAGE_SUPERRES, s);
+        ctx->launches++;
+        if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
+    }
+    return finish(ctx, s, host_key, msg);
+}
+
+int32_t vaco_av1_superres_upscale_picture_host(vaco_av1_ctx* ctx, const vaco_av1_picture* in,
+                                               const vaco_av1_picture* out,
+                                               const vaco_av1_superres_picture_config* cfg, int32_t* msg) {
+    if (!ctx || !in || !out || !cfg) return invalid(msg, VACO_AV1_MSG_NULL_ARGUMENT);
+    const int np = cfg->monochrome ? 1 : 3;
+    for (int k = 0; k < np; ++k)
+        if (in->width[k] < 0 || in->height[k] < 0 || (in->planes[k] && in->stride[k] < in->width[k]) ||
+            out->width[k] < 0 || out->height[k] < 0 || (out->width[k] > 0 && out->height[k] > 0 && !out->planes[k]))
+            return invalid(msg, VACO_AV1_MSG_FRAME_GEOMETRY);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaSuccess;
+    vaco_av1_picture din, dout;
+    if (!stage_picture_in(ctx, in, np, S_H_IN0, &din, s, &e)) return cuda_fail(ctx, e, msg);
+    if (!alloc_picture(ctx, out, np, S_H_OUT0, &dout, &e)) return cuda_fail(ctx, e, msg);
+    for (int k = 0; k < np; ++k)
+        if (!in->planes[k]) din.planes[k] = nullptr;  // keeps vaco's missing-plane error
+    int32_t st = vaco_av1_superres_upscale_picture_dev(ctx, s, &din, &dout, cfg, msg);
+    if (st != VACO_AV1_OK) return st;
+    e = copy_picture_out(&dout, out, np, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
     return VACO_AV1_OK;

@@ -24,6 +24,7 @@
 //   the vertical pass must run.  Vertical edges read columns [X-7, X+6].
 // The staged region is [x0-8, x0+tw+8) x [y0-8, y0+th+8).
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "cdef_core.cuh"
@@ -719,18 +720,22 @@ size_t build_dbcdef_args(const DbCdefLaunch& L, void* out) {
     return off * sizeof(uint16_t);
 }
 
+// Per-device caches, shared by every host thread that launches: atomics, so
+// concurrent first launches on a device only repeat idempotent set-up.
+std::atomic<unsigned long long> g_attr_devices{0};
+std::atomic<int> g_sm_counts[64];
+
 cudaError_t dbcdef_kernel_attributes() {
-    static unsigned long long attr_devices = 0;
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 64 && !(attr_devices & (1ull << dev))) {
+    if (dev < 64 && !(g_attr_devices.load(std::memory_order_acquire) & (1ull << dev))) {
         cudaError_t e = cudaFuncSetAttribute(dbcdef_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(dbcdef_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(dbcdef_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
         if (e != cudaSuccess) return e;
-        attr_devices |= 1ull << dev;
+        g_attr_devices.fetch_or(1ull << dev, std::memory_order_release);
     }
     return cudaSuccess;
 }
@@ -743,12 +748,13 @@ cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
     dim3 grid(div_up(L.info.mi_cols, 16), div_up(L.info.mi_rows, 16));
     // 3 CTAs per SM once the frame has more than 2.5 waves of 4 per SM
     // (measured best on 4K and 2880-wide frames; 4 on 1080p and 2560-wide).
-    static int sm_counts[64] = {};
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64) {
-        if (!sm_counts[dev]) cudaDeviceGetAttribute(&sm_counts[dev], cudaDevAttrMultiProcessorCount, dev);
-        if (sm_counts[dev] > 0) sms = sm_counts[dev];
+        int n = g_sm_counts[dev].load(std::memory_order_relaxed);
+        if (n <= 0 && cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0)
+            g_sm_counts[dev].store(n, std::memory_order_relaxed);
+        if (n > 0) sms = n;
     }
     if ((long)grid.x * grid.y * 2 > 5L * 4 * sms)
         dbcdef_kernel<3><<<grid, kThreads, smem, stream>>>(a);

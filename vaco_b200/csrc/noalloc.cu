@@ -1,8 +1,12 @@
 // noalloc.cu -- the post-filter chain without any device allocation.
 //
-// vaco_av1_postfilter_frame_noalloc() runs the same kernels as
-// vaco_av1_postfilter_frame_dev(), but it needs no context and it allocates
-// nothing.  It serves callers that cannot call cudaMalloc.  One example is a
+// vaco_av1_postfilter_frame_noalloc() runs the same chain as
+// vaco_av1_postfilter_frame_dev(), with the same results, but it needs no
+// context and it allocates nothing.  It runs the per-stage kernels
+// (deblocking passes, CDEF, superres, restoration) rather than the fused
+// deblock+CDEF kernel: they keep the whole deblocked picture, which is what
+// the fixed array holds, instead of the context's separate stripe-row
+// buffer.  It serves callers that cannot call cudaMalloc.  One example is a
 // decoder plugin inside a host application that owns all device memory
 // through its own pool and forbids plugins from allocating.  Another is a
 // real-time path where an allocation's implicit device-wide synchronization
@@ -16,8 +20,13 @@
 //     256 bytes for the status word.  Every GPU that loads this library holds
 //     it until the process exits.  A frame whose intermediates do not fit is
 //     rejected with VACO_AV1_LIMIT_EXCEEDED / VACO_AV1_MSG_SCRATCH_LIMIT.
-//     That covers e.g. up to 1920x1088 4:2:0 without superres and
-//     1280x720 with superres.
+//     A frame needs, per plane, two pictures at the Mi-padded size and,
+//     with superres, one or (when restoration runs) two more at the
+//     upscaled size, each row pitch rounded up to 64 samples.  So a
+//     1920-wide 4:2:0 frame fits up to 1456 rows without superres (1920x1088
+//     with room to spare, 1920x1464 does not), and with superres and
+//     restoration 1024x720 -> 1280x720 fits while 1440x1080 -> 1920x1080
+//     does not.
 //   - All calls in the process share the array, which keeps the contents of
 //     the last call.  Every call rewrites the intermediates in full and
 //     resets the status word before its first kernel.  Calls whose GPU work
@@ -86,7 +95,9 @@ struct Carver {
 bool job_geometry_ok(const vaco_av1_frame_job& j) {
     const vaco_av1_frame_info& i = j.info;
     if (i.mi_rows <= 0 || i.mi_cols <= 0 || i.mi_rows > (1 << 15) || i.mi_cols > (1 << 15)) return false;
-    if (i.subsampling_x < 0 || i.subsampling_x > 1 || i.subsampling_y < 0 || i.subsampling_y > 1) return false;
+    // 4:4:0 is refused as the context entry points refuse it: AV1 cannot
+    // signal it, and the chain's tile layout assumes it away.
+    if (!av1_subsampling_ok(i.subsampling_x, i.subsampling_y)) return false;
     if (i.coded_width <= 0 || i.coded_height <= 0) return false;
     if (i.mi_cols != 2 * ((i.coded_width + 7) >> 3) || i.mi_rows != 2 * ((i.coded_height + 7) >> 3)) return false;
     if (i.upscaled_width < i.coded_width) return false;

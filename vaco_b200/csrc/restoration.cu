@@ -24,6 +24,7 @@
 // Thread mappings put consecutive lanes on consecutive columns, so shared
 // memory reads are conflict-free and global writes coalesce.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "common.cuh"
@@ -665,18 +666,21 @@ int build_lr_args(const LrPlane* planes, int count, int bit_depth, void* out) {
 }
 
 // The opt-in above 48 KB of dynamic shared memory is a per-device attribute.
+// Atomic, as several host threads may launch on a device at once (a repeated
+// cudaFuncSetAttribute is harmless).
+std::atomic<unsigned long long> g_lr_attr_devices{0};
+
 cudaError_t lr_kernel_attributes() {
-    static unsigned long long attr_devices = 0;
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 64 && !(attr_devices & (1ull << dev))) {
+    if (dev < 64 && !(g_lr_attr_devices.load(std::memory_order_acquire) & (1ull << dev))) {
         cudaError_t e = cudaFuncSetAttribute(restoration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)kLrSmem);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(restoration_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)kLrSmem);
         if (e != cudaSuccess) return e;
-        attr_devices |= 1ull << dev;
+        g_lr_attr_devices.fetch_or(1ull << dev, std::memory_order_release);
     }
     return cudaSuccess;
 }

@@ -42,6 +42,7 @@ struct SlotBuffers {
     vaco_av1_frame_job job;  // device pointers of this frame slot
     std::vector<void*> allocations;
     bool in_flight = false;
+    cudaEvent_t uploaded = nullptr;  // recorded after a submit_host's input copies
 };
 
 struct StreamState {
@@ -59,6 +60,7 @@ struct Pending {
     vaco_av1_frame_job job;
     int64_t scratch;
     Clock::time_point submitted;
+    cudaEvent_t upload = nullptr;  // the launch waits for it (submit_host)
 };
 
 struct TicketState {
@@ -76,6 +78,10 @@ struct LaunchSlot {
     BatchPending pending;
 };
 
+// Default bound of the server's host waits (a slot's backpressure in submit,
+// a stream's in-flight frames in close_stream), in 1 ms polls.
+constexpr int kDefaultWaitPolls = 10000;
+
 size_t plane_bytes(int w, int h) { return align_up((size_t)align_up((size_t)std::max(w, 1), 64) * std::max(h, 1) * 2, 256); }
 
 }  // namespace
@@ -90,6 +96,8 @@ struct vaco_av1_server {
     std::vector<LaunchSlot> launch;
     uint64_t next_ticket = 1;
     int64_t resident = 0, stream_budget = 0, scratch_share = 0;
+    cudaStream_t upload_stream = nullptr;  // host->device copies of submit_host
+    int wait_polls = kDefaultWaitPolls;      // bound of submit / close_stream waits
     vaco_av1_server_stats stats{};
     bool stop = false;
     std::thread worker;
@@ -148,7 +156,13 @@ struct vaco_av1_server {
                 for (size_t i = 0; i < ls.jobs.size(); ++i) ls.table[i] = ls.jobs[i].job;
                 // the launch slot belongs to this thread: submitters may proceed meanwhile
                 lk.unlock();
-                int32_t st = batch_enqueue(ls.ctx, ls.ctx->stream, ls.table.data(), (int)ls.table.size(), &ls.pending);
+                // frames submitted with their inputs: the launch follows their copies
+                cudaError_t we = cudaSuccess;
+                for (const Pending& j : ls.jobs)
+                    if (j.upload && we == cudaSuccess) we = cudaStreamWaitEvent(ls.ctx->stream, j.upload, 0);
+                int32_t st = we == cudaSuccess ? batch_enqueue(ls.ctx, ls.ctx->stream, ls.table.data(),
+                                                               (int)ls.table.size(), &ls.pending)
+                                               : VACO_AV1_DEVICE_ERROR;
                 cudaError_t e = st == VACO_AV1_OK ? cudaEventRecord(ls.done, ls.ctx->stream) : cudaErrorUnknown;
                 lk.lock();
                 ++stats.batches;
@@ -176,8 +190,10 @@ struct vaco_av1_server {
 namespace {
 
 void free_stream(StreamState& s) {
-    for (SlotBuffers& b : s.slots)
+    for (SlotBuffers& b : s.slots) {
         for (void* p : b.allocations) cudaFree(p);
+        if (b.uploaded) cudaEventDestroy(b.uploaded);
+    }
     s.slots.clear();
     s.open = false;
 }
@@ -186,18 +202,23 @@ void free_stream(StreamState& s) {
 
 extern "C" int32_t vaco_av1_server_create(const vaco_av1_server_config* config, vaco_av1_server** out) {
     if (!config || !out || config->max_batch_frames < 1 || config->inflight_batches < 1 ||
-        config->inflight_batches > 8 || config->memory_budget_bytes <= 0)
+        config->inflight_batches > 8 || config->memory_budget_bytes <= 0 || config->host_wait_ms < 0)
         return VACO_AV1_INVALID_DATA;
     *out = nullptr;
     if (cudaSetDevice(config->device) != cudaSuccess) return VACO_AV1_DEVICE_ERROR;
     vaco_av1_server* s = new vaco_av1_server();
     s->cfg = *config;
+    if (config->host_wait_ms > 0) s->wait_polls = config->host_wait_ms;
     // a quarter of the budget is reserved for batch scratch, shared by the launch slots
     const int64_t scratch_total = config->memory_budget_bytes / 4;
     s->scratch_share = scratch_total / config->inflight_batches;
     s->stream_budget = config->memory_budget_bytes - scratch_total;
     s->stats.scratch_bytes = scratch_total;
     s->launch.resize(config->inflight_batches);
+    if (cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        vaco_av1_server_destroy(s);
+        return VACO_AV1_DEVICE_ERROR;
+    }
     for (LaunchSlot& ls : s->launch) {
         if (vaco_av1_ctx_create(config->device, &ls.ctx) != VACO_AV1_OK ||
             cudaEventCreateWithFlags(&ls.done, cudaEventDisableTiming) != cudaSuccess) {
@@ -231,6 +252,7 @@ extern "C" void vaco_av1_server_destroy(vaco_av1_server* s) {
         if (ls.ctx) vaco_av1_ctx_destroy(ls.ctx);
     }
     for (StreamState& st : s->streams) free_stream(st);
+    if (s->upload_stream) cudaStreamDestroy(s->upload_stream);
     delete s;
 }
 
@@ -324,7 +346,8 @@ extern "C" int32_t vaco_av1_server_open_stream(vaco_av1_server* s, const vaco_av
         j.cdef_idx = static_cast<const int32_t*>(alloc(b, nidx * 4));
         j.cdef_stride = (i.mi_cols + 15) / 16;
         j.cdef_count = (int32_t)nidx;
-        ok = ok && j.tx_luma && j.tx_chroma && j.skip && j.lvl_map && j.cdef_idx;
+        ok = ok && j.tx_luma && j.tx_chroma && j.skip && j.lvl_map && j.cdef_idx &&
+             cudaEventCreateWithFlags(&b.uploaded, cudaEventDisableTiming) == cudaSuccess;
         if (!ok) {
             free_stream(st);
             if (msg) *msg = VACO_AV1_MSG_CUDA;
@@ -352,12 +375,16 @@ extern "C" int32_t vaco_av1_server_close_stream(vaco_av1_server* s, int32_t id) 
     if (!s) return VACO_AV1_INVALID_DATA;
     std::unique_lock<std::mutex> lk(s->mu);
     if (id < 0 || id >= (int)s->streams.size() || !s->streams[id].open) return VACO_AV1_INVALID_DATA;
-    // wait (bounded polls) until none of its slots is in flight
-    for (;;) {
+    // Wait until none of its slots is in flight: bounded polls, then
+    // VACO_AV1_TIMEOUT with the stream left open (its frames still complete
+    // and a later close succeeds).
+    for (int waited = 0;; ++waited) {
         bool busy = false;
         for (const SlotBuffers& b : s->streams[id].slots) busy = busy || b.in_flight;
         if (!busy) break;
+        if (waited >= s->wait_polls) return VACO_AV1_TIMEOUT;
         s->cv_done.wait_for(lk, std::chrono::milliseconds(1));
+        if (id >= (int)s->streams.size() || !s->streams[id].open) return VACO_AV1_INVALID_DATA;
     }
     cudaSetDevice(s->cfg.device);
     s->resident -= s->streams[id].bytes;
@@ -375,18 +402,27 @@ extern "C" int32_t vaco_av1_server_slot(vaco_av1_server* s, int32_t id, int32_t 
     return VACO_AV1_OK;
 }
 
-extern "C" int32_t vaco_av1_server_submit(vaco_av1_server* s, int32_t id, int32_t slot, const vaco_av1_frame_job* params,
-                                          uint64_t* ticket) {
-    if (!s || !params || !ticket) return VACO_AV1_INVALID_DATA;
-    std::unique_lock<std::mutex> lk(s->mu);
+namespace {
+
+// Waits while slot `slot` of stream `id` is still in flight (backpressure,
+// bounded) and reserves it for the caller.  `lk` holds the server mutex.
+int32_t reserve_slot(vaco_av1_server* s, std::unique_lock<std::mutex>& lk, int32_t id, int32_t slot) {
     if (id < 0 || id >= (int)s->streams.size() || !s->streams[id].open) return VACO_AV1_INVALID_DATA;
     if (slot < 0 || slot >= (int)s->streams[id].slots.size()) return VACO_AV1_INVALID_DATA;
-    // Backpressure: a slot still in flight is waited for (bounded polls, 10 s).
     for (int waited = 0; s->streams[id].slots[slot].in_flight; ++waited) {
-        if (waited >= 10000) return VACO_AV1_TIMEOUT;
+        if (waited >= s->wait_polls) return VACO_AV1_TIMEOUT;
         s->cv_done.wait_for(lk, std::chrono::milliseconds(1));
         if (id >= (int)s->streams.size() || !s->streams[id].open) return VACO_AV1_INVALID_DATA;
     }
+    s->streams[id].slots[slot].in_flight = true;
+    return VACO_AV1_OK;
+}
+
+// Queues a reserved slot with the frame-level parameters of `params`; the
+// launch that takes it first waits for `upload` when that is set.  `lk`
+// holds the server mutex.
+uint64_t queue_slot(vaco_av1_server* s, int32_t id, int32_t slot, const vaco_av1_frame_job* params,
+                    cudaEvent_t upload) {
     StreamState& st = s->streams[id];
     Pending p;
     p.ticket = s->next_ticket++;
@@ -405,12 +441,94 @@ extern "C" int32_t vaco_av1_server_submit(vaco_av1_server* s, int32_t id, int32_
     if (!params->lvl_map) p.job.lvl_map = nullptr;
     p.scratch = st.scratch_estimate;
     p.submitted = Clock::now();
-    st.slots[slot].in_flight = true;
+    p.upload = upload;
     s->tickets.emplace(p.ticket, TicketState{});
     s->pending.push_back(p);
     ++s->stats.submitted;
-    *ticket = p.ticket;
     s->cv_work.notify_one();
+    return p.ticket;
+}
+
+// Enqueues the copies of a host frame (planes, restoration units, side
+// information) into the device buffers `d` of a slot on `stream`.
+cudaError_t enqueue_upload(const vaco_av1_frame_job& d, const vaco_av1_frame_job* host, cudaStream_t stream) {
+    const vaco_av1_frame_info& i = d.info;
+    const int np = i.monochrome ? 1 : 3;
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < np && e == cudaSuccess; ++k) {
+        if (d.src.width[k] > 0 && d.src.height[k] > 0)
+            e = cudaMemcpy2DAsync(d.src.planes[k], (size_t)d.src.stride[k] * 2, host->src.planes[k],
+                                  (size_t)host->src.stride[k] * 2, (size_t)d.src.width[k] * 2, d.src.height[k],
+                                  cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess && d.lr_units[k] && host->lr_units[k] && host->lr_unit_count[k] == d.lr_unit_count[k])
+            e = cudaMemcpyAsync(const_cast<vaco_av1_lr_unit*>(d.lr_units[k]), host->lr_units[k],
+                                sizeof(vaco_av1_lr_unit) * d.lr_unit_count[k], cudaMemcpyHostToDevice, stream);
+    }
+    const size_t cells = (size_t)i.mi_rows * i.mi_cols;
+    const size_t ccells = (size_t)((i.mi_rows + i.subsampling_y) >> i.subsampling_y) *
+                          ((i.mi_cols + i.subsampling_x) >> i.subsampling_x);
+    auto up = [&](const void* dst, const void* src, size_t bytes) {
+        if (e == cudaSuccess && src && bytes)
+            e = cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, stream);
+    };
+    up(d.tx_luma, host->tx_luma, cells);
+    if (np > 1) up(d.tx_chroma, host->tx_chroma, ccells);
+    up(d.skip, host->skip, cells);
+    up(d.lvl_map, host->lvl_map, cells * 4);
+    if (host->cdef_idx && host->cdef_count == d.cdef_count)
+        up(d.cdef_idx, host->cdef_idx, sizeof(int32_t) * d.cdef_count);
+    return e;
+}
+
+// A host frame must match the slot's geometry and carry every plane.
+bool host_frame_fits(const vaco_av1_frame_job& d, const vaco_av1_frame_job* host) {
+    const vaco_av1_frame_info& i = d.info;
+    if (host->info.mi_rows != i.mi_rows || host->info.mi_cols != i.mi_cols || host->info.bit_depth != i.bit_depth)
+        return false;
+    const int np = i.monochrome ? 1 : 3;
+    for (int k = 0; k < np; ++k)
+        if (!host->src.planes[k] || host->src.stride[k] < d.src.width[k]) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" int32_t vaco_av1_server_submit(vaco_av1_server* s, int32_t id, int32_t slot, const vaco_av1_frame_job* params,
+                                          uint64_t* ticket) {
+    if (!s || !params || !ticket) return VACO_AV1_INVALID_DATA;
+    std::unique_lock<std::mutex> lk(s->mu);
+    const int32_t st = reserve_slot(s, lk, id, slot);
+    if (st != VACO_AV1_OK) return st;
+    *ticket = queue_slot(s, id, slot, params, nullptr);
+    return VACO_AV1_OK;
+}
+
+extern "C" int32_t vaco_av1_server_submit_host(vaco_av1_server* s, int32_t id, int32_t slot,
+                                               const vaco_av1_frame_job* host, uint64_t* ticket) {
+    if (!s || !host || !ticket) return VACO_AV1_INVALID_DATA;
+    std::unique_lock<std::mutex> lk(s->mu);
+    int32_t st = reserve_slot(s, lk, id, slot);
+    if (st != VACO_AV1_OK) return st;
+    const vaco_av1_frame_job d = s->streams[id].slots[slot].job;
+    const cudaEvent_t ev = s->streams[id].slots[slot].uploaded;
+    if (!host_frame_fits(d, host)) {
+        s->streams[id].slots[slot].in_flight = false;
+        s->cv_done.notify_all();
+        return VACO_AV1_INVALID_DATA;
+    }
+    // The reserved slot keeps close_stream and other submits away while the
+    // copies are enqueued without the lock.
+    lk.unlock();
+    cudaSetDevice(s->cfg.device);
+    cudaError_t e = enqueue_upload(d, host, s->upload_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev, s->upload_stream);
+    lk.lock();
+    if (e != cudaSuccess) {
+        s->streams[id].slots[slot].in_flight = false;
+        s->cv_done.notify_all();
+        return VACO_AV1_DEVICE_ERROR;
+    }
+    *ticket = queue_slot(s, id, slot, host, ev);
     return VACO_AV1_OK;
 }
 
@@ -455,31 +573,10 @@ extern "C" int32_t vaco_av1_server_upload(vaco_av1_server* s, int32_t id, int32_
     if (!s || !host) return VACO_AV1_INVALID_DATA;
     vaco_av1_frame_job d;
     if (vaco_av1_server_slot(s, id, slot, &d) != VACO_AV1_OK) return VACO_AV1_INVALID_DATA;
-    const vaco_av1_frame_info& i = d.info;
-    if (host->info.mi_rows != i.mi_rows || host->info.mi_cols != i.mi_cols || host->info.bit_depth != i.bit_depth)
-        return VACO_AV1_INVALID_DATA;
+    if (!host_frame_fits(d, host)) return VACO_AV1_INVALID_DATA;
     cudaSetDevice(s->cfg.device);
-    const int np = i.monochrome ? 1 : 3;
-    cudaError_t e = cudaSuccess;
-    for (int k = 0; k < np && e == cudaSuccess; ++k) {
-        if (!host->src.planes[k]) return VACO_AV1_INVALID_DATA;
-        e = copy_plane(d.src.planes[k], d.src.stride[k], host->src.planes[k], host->src.stride[k], d.src.width[k],
-                       d.src.height[k], cudaMemcpyHostToDevice);
-        if (e == cudaSuccess && d.lr_units[k] && host->lr_units[k] && host->lr_unit_count[k] == d.lr_unit_count[k])
-            e = cudaMemcpy(const_cast<vaco_av1_lr_unit*>(d.lr_units[k]), host->lr_units[k],
-                           sizeof(vaco_av1_lr_unit) * d.lr_unit_count[k], cudaMemcpyHostToDevice);
-    }
-    const size_t cells = (size_t)i.mi_rows * i.mi_cols;
-    const size_t ccells = (size_t)((i.mi_rows + i.subsampling_y) >> i.subsampling_y) *
-                          ((i.mi_cols + i.subsampling_x) >> i.subsampling_x);
-    auto up = [&](const void* dst, const void* src, size_t bytes) {
-        if (e == cudaSuccess && src && bytes) e = cudaMemcpy(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice);
-    };
-    up(d.tx_luma, host->tx_luma, cells);
-    if (np > 1) up(d.tx_chroma, host->tx_chroma, ccells);
-    up(d.skip, host->skip, cells);
-    up(d.lvl_map, host->lvl_map, cells * 4);
-    if (host->cdef_idx && host->cdef_count == d.cdef_count) up(d.cdef_idx, host->cdef_idx, sizeof(int32_t) * d.cdef_count);
+    cudaError_t e = enqueue_upload(d, host, s->upload_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->upload_stream);
     return e == cudaSuccess ? VACO_AV1_OK : VACO_AV1_DEVICE_ERROR;
 }
 

@@ -111,6 +111,33 @@ class Context:
         _check(self, st, m)
         return out
 
+    def upscale_picture(self, planes, config: abi.SuperresPictureConfig) -> List[np.ndarray]:
+        """superres::upscale_picture through the host entry point: Mi-padded
+        planes (None for an absent chroma plane) in, upscaled planes out."""
+        n = 1 if config.monochrome else 3
+        ins = [None if p is None else np.ascontiguousarray(p, np.uint16) for p in planes]
+        outs = []
+        for k in range(n):
+            sx = config.subsampling_x if k else 0
+            sy = config.subsampling_y if k else 0
+            w = -(-config.upscaled_width // (1 << sx))
+            h = -(-config.coded_height // (1 << sy))
+            outs.append(np.zeros((max(h, 0), max(w, 0)), np.uint16))
+        pin, pout = abi.Picture(), abi.Picture()
+        for k in range(n):
+            if ins[k] is not None:
+                pin.planes[k] = ins[k].ctypes.data
+                pin.height[k], pin.width[k] = ins[k].shape
+                pin.stride[k] = ins[k].shape[1]
+            pout.planes[k] = outs[k].ctypes.data if outs[k].size else None
+            pout.height[k], pout.width[k] = outs[k].shape
+            pout.stride[k] = max(outs[k].shape[1], 1)
+        m = C.c_int32()
+        st = lib().vaco_av1_superres_upscale_picture_host(self.handle, C.byref(pin), C.byref(pout), C.byref(config),
+                                                          C.byref(m))
+        _check(self, st, m)
+        return outs
+
     def restore_plane(self, before: np.ndarray, after: np.ndarray, width: int, height: int, bit_depth: int,
                       unit_size: int, subsampling_y: bool, units: np.ndarray) -> np.ndarray:
         before = np.ascontiguousarray(before, np.uint16)

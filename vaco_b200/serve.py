@@ -29,7 +29,7 @@ class ServerConfig(C.Structure):
         ("device", C.c_int32),
         ("max_batch_frames", C.c_int32),
         ("inflight_batches", C.c_int32),
-        ("reserved", C.c_int32),
+        ("host_wait_ms", C.c_int32),
         ("memory_budget_bytes", C.c_int64),
     ]
 
@@ -54,9 +54,10 @@ def _declare():
 class Server:
     """Handle on vaco_av1_server."""
 
-    def __init__(self, device=0, max_batch_frames=64, inflight_batches=3, memory_budget_bytes=40 << 30):
+    def __init__(self, device=0, max_batch_frames=64, inflight_batches=3, memory_budget_bytes=40 << 30,
+                 host_wait_ms=0):
         self.l = _declare()
-        cfg = ServerConfig(device, max_batch_frames, inflight_batches, 0, memory_budget_bytes)
+        cfg = ServerConfig(device, max_batch_frames, inflight_batches, host_wait_ms, memory_budget_bytes)
         h = C.c_void_p()
         st = self.l.vaco_av1_server_create(C.byref(cfg), C.byref(h))
         if st != abi.OK:
@@ -98,6 +99,24 @@ class Server:
             raise RuntimeError(f"submit refused: {st}")
         return t.value
 
+    def try_submit(self, sid: int, slot: int, params: abi.FrameJob):
+        """submit() returning (status, ticket) instead of raising."""
+        t = C.c_uint64()
+        st = self.l.vaco_av1_server_submit(self.h, sid, slot, C.byref(params), C.byref(t))
+        return st, t.value
+
+    def submit_host(self, sid: int, slot: int, host: abi.FrameJob) -> int:
+        """Queue slot `slot` with its inputs copied from the host frame job
+        `host` (host pointers; they must stay valid until wait returns)."""
+        t = C.c_uint64()
+        st = self.l.vaco_av1_server_submit_host(self.h, sid, slot, C.byref(host), C.byref(t))
+        if st != abi.OK:
+            raise RuntimeError(f"submit_host refused: {st}")
+        return t.value
+
+    def close_stream(self, sid: int) -> int:
+        return self.l.vaco_av1_server_close_stream(self.h, sid)
+
     def wait(self, ticket: int, timeout_ms: int = -1):
         msg, lat = C.c_int32(0), C.c_double(0)
         st = self.l.vaco_av1_server_wait(self.h, ticket, timeout_ms, C.byref(msg), C.byref(lat))
@@ -128,12 +147,16 @@ def _percentile(xs, q):
     return xs[min(len(xs) - 1, int(round(q / 100.0 * (len(xs) - 1))))]
 
 
-def run_load(server: Server, streams, rate_mult: float, seconds: float, fps: float = 30.0, seed: int = 0):
+def run_load(server: Server, streams, rate_mult: float, seconds: float, fps: float = 30.0, seed: int = 0,
+             upload: bool = False):
     """Poisson arrivals per stream at fps*rate_mult for `seconds`.
 
     A frame's latency is measured from its scheduled arrival: the submitter's
     lag behind the schedule, any backpressure wait inside submit (slot still
-    in flight) and the server's submit-to-completion time."""
+    in flight) and the server's submit-to-completion time.  With `upload`,
+    every frame arrives in host memory (pinned) and goes in through
+    vaco_av1_server_submit_host, so its latency also covers the copy of its
+    inputs to the device; otherwise the frames are already resident."""
     rng = random.Random(seed)
     arrivals = []
     for s_idx, st in enumerate(streams):
@@ -173,7 +196,10 @@ def run_load(server: Server, streams, rate_mult: float, seconds: float, fps: flo
         st = streams[s_idx]
         slot = next_slot[s_idx]
         next_slot[s_idx] = (slot + 1) % st["buffers"]
-        ticket = server.submit(st["id"], slot, st["params"][slot])
+        if upload:
+            ticket = server.submit_host(st["id"], slot, st["host_jobs"][slot])
+        else:
+            ticket = server.submit(st["id"], slot, st["params"][slot])
         queued_ms = max(0.0, (time.perf_counter() - t0) - t) * 1e3
         with lock:
             inflight.append((ticket, st["pixels"], queued_ms))
@@ -181,7 +207,7 @@ def run_load(server: Server, streams, rate_mult: float, seconds: float, fps: flo
     th.join()
     wall = time.perf_counter() - t0
     return {
-        "rate_x_realtime": rate_mult, "offered_fps": round(len(streams) * fps * rate_mult, 1),
+        "rate_x_realtime": rate_mult, "uploads": upload, "offered_fps": round(len(streams) * fps * rate_mult, 1),
         "frames": len(latencies), "errors": errors, "seconds": round(wall, 2),
         "mpixel_s": round(pixels / wall / 1e6, 1),
         "p50_ms": round(_percentile(latencies, 50), 3) if latencies else None,
@@ -190,9 +216,21 @@ def run_load(server: Server, streams, rate_mult: float, seconds: float, fps: flo
     }
 
 
-def saturation(server: Server, streams, rounds: int = 20):
+def saturation(server: Server, streams, rounds: int = 20, upload: bool = False):
     """Every slot of every stream submitted at once, round after round, with
-    the bulk entry points: the served path's peak Mpixel/s."""
+    the bulk entry points: the served path's peak Mpixel/s.  With `upload`
+    every frame goes in from pinned host memory through submit_host."""
+    if upload:
+        px = sum(st["pixels"] * st["buffers"] for st in streams)
+        t0 = time.perf_counter()
+        for _ in range(rounds):
+            tickets = [server.submit_host(st["id"], b, st["host_jobs"][b]) for st in streams
+                       for b in range(st["buffers"])]
+            for t in tickets:
+                assert server.wait(t, -1)[0] == abi.OK
+        wall = time.perf_counter() - t0
+        return {"frames": rounds * len(tickets), "mpixel_s": round(rounds * px / wall / 1e6, 1),
+                "seconds": round(wall, 3), "uploads": True}
     ids, slots, params, px = [], [], [], 0
     for st in streams:
         for b in range(st["buffers"]):
@@ -213,24 +251,30 @@ def saturation(server: Server, streams, rounds: int = 20):
         st = l.vaco_av1_server_wait_many(server.h, n, tickets, -1, None, None, None)
         assert st == abi.OK, st
     wall = time.perf_counter() - t0
-    return {"frames": rounds * n, "mpixel_s": round(rounds * px / wall / 1e6, 1), "seconds": round(wall, 3)}
+    return {"frames": rounds * n, "mpixel_s": round(rounds * px / wall / 1e6, 1), "seconds": round(wall, 3),
+            "uploads": False}
 
 
 def plain_dropin_mixed(device=0, frames_per_res=4, rounds=8):
     """The plain one-frame-per-call drop-in on the same mixed-resolution
-    frames: vaco_av1_postfilter_frame_host, H2D + D2H every call, one frame
-    at a time.  Inputs and outputs sit in pinned, preallocated host buffers
-    (the drop-in's best case), so the served/plain ratio is not inflated by
-    pageable copies.  Mpixel/s."""
-    from .gpu import Context
+    frames, two ways:
+      with copies  vaco_av1_postfilter_frame_host: H2D + D2H every call, one
+                   frame at a time, from pinned preallocated host buffers (the
+                   drop-in's best case, so the served/plain ratio is not
+                   inflated by pageable copies);
+      resident     vaco_av1_postfilter_frame_dev on device-resident frames,
+                   one call per frame, each synchronizing for its status.
+    Mpixel/s of each."""
+    from .gpu import Context, DeviceFrame
 
     ctx = Context(device)
-    jobs, px_per_round = [], 0
+    jobs, frames, px_per_round = [], [], 0
     for wl, _ in synth.BATCH_MIX:
         for i in range(frames_per_res):
             f = synth.make_frame(wl, synth.seed_for(4, 7000 + len(jobs)))
             pf, outs, job = pinned_copy(f)
             jobs.append((pf, outs, job))
+            frames.append(f)
             px_per_round += f.output_pixels
     l, m = lib(), C.c_int32()
     for _, _, job in jobs:  # warm: every frame size once (scratch reaches its final size)
@@ -242,12 +286,22 @@ def plain_dropin_mixed(device=0, frames_per_res=4, rounds=8):
             if st != abi.OK:
                 raise RuntimeError(f"host postfilter failed: {st}")
     wall = time.perf_counter() - t0
+    devs = [DeviceFrame(f, device) for f in frames]
+    for d in devs:
+        ctx.postfilter_frame_dev(d)
+    t1 = time.perf_counter()
+    for _ in range(rounds):
+        for d in devs:
+            ctx.postfilter_frame_dev(d)
+    wall_dev = time.perf_counter() - t1
     ctx.close()
     return {"frames": rounds * len(jobs), "mpixel_s": round(rounds * px_per_round / wall / 1e6, 1),
-            "entry": "vaco_av1_postfilter_frame_host (pinned host buffers)"}
+            "entry": "vaco_av1_postfilter_frame_host (pinned host buffers)",
+            "resident_mpixel_s": round(rounds * px_per_round / wall_dev / 1e6, 1),
+            "resident_entry": "vaco_av1_postfilter_frame_dev, one synchronous call per device-resident frame"}
 
 
-def build_streams(server: Server, per_res: int = 8, buffers: int = 4, base_seed: int = 9000):
+def build_streams(server: Server, per_res: int = 8, buffers: int = 4, base_seed: int = 9000, pinned: bool = False):
     streams = []
     for wl, _ in synth.BATCH_MIX:
         for i in range(per_res):
@@ -257,9 +311,52 @@ def build_streams(server: Server, per_res: int = 8, buffers: int = 4, base_seed:
                 raise RuntimeError(f"stream admission refused: {abi.MESSAGES.get(msg)}")
             for b, f in enumerate(frames):
                 server.upload(sid, b, f)
-            streams.append({"id": sid, "buffers": buffers, "pixels": frames[0].output_pixels,
-                            "params": [frame_params(f) for f in frames], "frames": frames, "workload": wl.name})
+            entry = {"id": sid, "buffers": buffers, "pixels": frames[0].output_pixels,
+                     "params": [frame_params(f) for f in frames], "frames": frames, "workload": wl.name}
+            if pinned:  # host copies for submit_host: arrays stay referenced by the entry
+                staged = [pinned_copy(f) for f in frames]
+                entry["pinned"] = staged
+                entry["host_jobs"] = [job for _, _, job in staged]
+            streams.append(entry)
     return streams
+
+
+SERVE_CONFIG = {"workload": "serve_32_streams", "streams": "8 x each of 640x360 8-bit, 1280x720 8-bit, "
+                "1920x1080 10-bit, 3840x2160 10-bit", "fps_per_stream": 30, "memory_budget_gb": 40,
+                "max_batch_frames": 64, "inflight_batches": 3, "buffers_per_stream": 4}
+
+
+def served(device: int, seconds: float, rates=(1.0, 2.0, 4.0), saturation_rounds: int = 20):
+    """Config 4 on one GPU: Poisson load at each rate for `seconds`, twice --
+    frames resident in their slots, and every frame uploaded from pinned host
+    memory inside its latency -- plus saturation both ways and the plain
+    one-frame-per-call drop-in on the same mixed frames."""
+    server = Server(device, max_batch_frames=64, inflight_batches=3)
+    try:
+        streams = build_streams(server, pinned=True)
+        saturation(server, streams, rounds=3)  # warm: first launches of every batch shape
+        saturation(server, streams, rounds=2, upload=True)
+        resident = [run_load(server, streams, m, seconds, seed=int(m * 10)) for m in rates]
+        uploaded = [run_load(server, streams, m, seconds, seed=int(m * 10) + 1, upload=True) for m in rates]
+        sat = saturation(server, streams, rounds=saturation_rounds)
+        sat_up = saturation(server, streams, rounds=max(2, saturation_rounds // 4), upload=True)
+        stats = server.stats()
+    finally:
+        server.close()
+    plain = plain_dropin_mixed(device)
+    return {
+        "config": dict(SERVE_CONFIG, seconds_per_rate=seconds),
+        "resident": resident, "with_uploads": uploaded,
+        "saturation": {"resident": sat, "with_uploads": sat_up},
+        "plain_dropin_mixed": plain,
+        "served_over_plain": {
+            "with_copies": round(sat_up["mpixel_s"] / plain["mpixel_s"], 2) if plain["mpixel_s"] else None,
+            "resident": round(sat["mpixel_s"] / plain["resident_mpixel_s"], 2) if plain["resident_mpixel_s"] else None,
+            "note": "saturation with uploads / plain host drop-in (both copy every frame); "
+                    "resident saturation / plain device-resident drop-in"},
+        "server": {"batches": int(stats.batches), "max_batch": int(stats.max_batch),
+                   "resident_gb": round(stats.resident_bytes / 2**30, 3)},
+    }
 
 
 def bench_main(args, world, rank, local):
@@ -268,24 +365,7 @@ def bench_main(args, world, rank, local):
 
     torch.cuda.set_device(local)
     seconds = float(getattr(args, "serve_seconds", 0) or 60.0)
-    server = Server(local, max_batch_frames=64, inflight_batches=3)
-    try:
-        streams = build_streams(server)
-        saturation(server, streams, rounds=3)  # warm: first launches of every batch shape
-        results = [run_load(server, streams, m, seconds, seed=int(m * 10)) for m in (1.0, 2.0, 4.0)]
-        sat = saturation(server, streams)
-        stats = server.stats()
-    finally:
-        server.close()
-    plain = plain_dropin_mixed(local)
+    res = served(local, seconds)
     if rank == 0:
-        print(json.dumps({
-            "metric": "AV1 post-filter served p50/p99 ms/frame and Mpixel/s", "mode": "serve",
-            "config": {"workload": "serve_32_streams", "streams": "8 x each of 640x360 8-bit, 1280x720 8-bit, "
-                       "1920x1080 10-bit, 3840x2160 10-bit", "fps_per_stream": 30, "seconds_per_rate": seconds,
-                       "memory_budget_gb": 40, "max_batch_frames": 64, "inflight_batches": 3},
-            "rates": results, "saturation": sat, "plain_dropin_mixed": plain,
-            "served_over_plain": round(sat["mpixel_s"] / plain["mpixel_s"], 2) if plain["mpixel_s"] else None,
-            "server": {"batches": stats.batches, "max_batch": stats.max_batch,
-                       "resident_gb": round(stats.resident_bytes / 2**30, 3)},
-        }), flush=True)
+        print(json.dumps(dict({"metric": "AV1 post-filter served p50/p99 ms/frame and Mpixel/s", "mode": "serve"},
+                              **res)), flush=True)
