@@ -224,6 +224,7 @@ pub struct Tuning {
     pub lr_ctas_per_sm: i32,
     pub use_graphs: i32,
     pub largest_first: i32,
+    pub dbcdef_threads: i32,
 }
 
 #[repr(C)]

@@ -406,6 +406,9 @@ typedef struct vaco_av1_tuning {
     int32_t lr_ctas_per_sm;      /* persistent CTAs per SM, restoration kernel (1..4) */
     int32_t use_graphs;          /* capture each batch composition once as a CUDA graph */
     int32_t largest_first;       /* queue the largest frames' tiles first */
+    int32_t dbcdef_threads;      /* threads per 64x64 tile of the deblock+CDEF kernel, in the
+                                    batched form and vaco_av1_postfilter_frame_dev: 256 or
+                                    128 (0 = 256) */
 } vaco_av1_tuning;
 
 VACO_AV1_API int32_t vaco_av1_ctx_set_tuning(vaco_av1_ctx* ctx, const vaco_av1_tuning* tuning);

@@ -27,8 +27,8 @@ _lib = None
 
 def build(force: bool = False) -> pathlib.Path:
     """Compile the oracle with its Makefile (g++ -O2)."""
-    src = HERE / "vaco_oracle.cpp"
-    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+    deps = [HERE / "vaco_oracle.cpp", HERE.parent / "include" / "vaco_av1_gpu.h"]
+    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max(d.stat().st_mtime for d in deps):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB_PATH
 

@@ -176,6 +176,7 @@ class Tuning(C.Structure):
         ("lr_ctas_per_sm", C.c_int32),
         ("use_graphs", C.c_int32),
         ("largest_first", C.c_int32),
+        ("dbcdef_threads", C.c_int32),
     ]
 
 

@@ -16,7 +16,7 @@ import sys
 
 ROOT = pathlib.Path(__file__).resolve().parent.parent
 TUNED = ROOT / "tuned"
-DEFAULT = {"dbcdef_ctas_per_sm": 3, "lr_ctas_per_sm": 4, "use_graphs": 1, "largest_first": 1}
+DEFAULT = {"dbcdef_ctas_per_sm": 3, "lr_ctas_per_sm": 4, "use_graphs": 1, "largest_first": 1, "dbcdef_threads": 256}
 
 
 def gpu_key() -> str:

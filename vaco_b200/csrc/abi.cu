@@ -907,6 +907,7 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
             L.cdef_count = job->cdef_count;
             L.cdef = cp;
             L.status = ctx->status;
+            L.threads = ctx->tuning.dbcdef_threads == 128 ? 128 : 256;
             e = launch_dbcdef(L, s);
             ctx->launches++;
             if (e != cudaSuccess) return cuda_fail(ctx, e, msg);

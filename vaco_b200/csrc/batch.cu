@@ -105,7 +105,8 @@ int32_t fail(vaco_av1_ctx* ctx, cudaError_t e, int32_t* statuses, int32_t* msgs,
 
 extern "C" int32_t vaco_av1_ctx_set_tuning(vaco_av1_ctx* ctx, const vaco_av1_tuning* t) {
     if (!ctx || !t) return VACO_AV1_INVALID_DATA;
-    if (t->dbcdef_ctas_per_sm < 1 || t->dbcdef_ctas_per_sm > 8 || t->lr_ctas_per_sm < 1 || t->lr_ctas_per_sm > 8)
+    if (t->dbcdef_ctas_per_sm < 1 || t->dbcdef_ctas_per_sm > 8 || t->lr_ctas_per_sm < 1 || t->lr_ctas_per_sm > 8 ||
+        !(t->dbcdef_threads == 0 || t->dbcdef_threads == 128 || t->dbcdef_threads == 256))
         return VACO_AV1_INVALID_DATA;
     ctx->tuning = *t;
     return VACO_AV1_OK;
@@ -358,7 +359,8 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
         cudaError_t r = cudaMemcpyAsync(dtab, htab, table_bytes, cudaMemcpyHostToDevice, s);
         if (r == cudaSuccess && !order.empty() && db_prefix[order.size()] > 0)
             r = launch_dbcdef_batch(dtab + off_db, reinterpret_cast<const int*>(dtab + off_db_prefix), (int)order.size(),
-                                    reinterpret_cast<int*>(dtab + off_queue), smem_db, grid_db, s);
+                                    reinterpret_cast<int*>(dtab + off_queue), smem_db, grid_db,
+                                    ctx->tuning.dbcdef_ctas_per_sm, ctx->tuning.dbcdef_threads, s);
         for (int i : order) {
             const FramePlan& F = plan[i];
             if (r != cudaSuccess || !F.superres) continue;

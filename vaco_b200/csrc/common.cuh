@@ -32,6 +32,38 @@ __device__ __forceinline__ void report_error(DeviceStatus* st, unsigned stage,
     atomicMin(&st->first_error, key);
 }
 
+// ---------------------------------------------------------------- overlapped launches
+//
+// The chain's kernels (fused deblock+CDEF, superres, restoration) are
+// launched with programmatic stream serialization: a kernel may be scheduled
+// while the kernel before it on the stream runs its last CTAs.  Each of them
+// calls overlap_prologue() before anything else.  It first lets the next
+// kernel on the stream be scheduled the same way, then waits until the
+// previous kernel has completed and its writes are visible, so every read and
+// write after it is ordered exactly as with a plain launch.  Only the launch
+// latency and the CTA start-up overlap the previous kernel's tail.  Without
+// the launch attribute both instructions are no-ops.
+__device__ __forceinline__ void overlap_prologue() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... Params, typename... Args>
+inline cudaError_t launch_overlapped(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                                     cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // ---------------------------------------------------------------- planes
 
 struct DevPlane {

@@ -23,6 +23,9 @@
 //   [y0-7, y0+th+7) for luma and [y0-3, y0+th+3) for chroma, which is where
 //   the vertical pass must run.  Vertical edges read columns [X-7, X+6].
 // The staged region is [x0-8, x0+tw+8) x [y0-8, y0+th+8).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cstring>
@@ -111,8 +114,53 @@ struct DbCdefArgs {
     size_t plane_off[3];        // shared-memory offset (samples) of each staged plane
 };
 
-// CDEF output of one plane tile from the staged (deblocked) samples: warp w
-// filters block row w; lane l owns pixel pairs at tile column 2*(l % ppr),
+// Tensor maps of a frame's input planes for staging interior tiles with TMA
+// (use == 0: every tile stages with cp.async).  A kernel parameter, so the
+// maps sit in parameter space where the tensor copies read them.
+struct alignas(64) DbCdefTma {
+    CUtensorMap map[3];
+    int use;
+};
+
+// Bound of the wait for a tile's tensor copies: try_wait suspends for a
+// system-dependent time per call, so this is far beyond any copy's latency.
+constexpr int kTmaWaitIters = 1 << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// One 2-D box of `map` with its first element at (x, y) into shared memory
+// at `dst` (128-byte aligned), completing on `bar`.  x * 2 bytes is a
+// multiple of 16 (x is a multiple of 8 samples) and the whole box lies inside
+// the plane; the source is this GPU's own memory and no multicast is used.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// CDEF output of one plane tile from the staged (deblocked) samples: one warp
+// filters block row br; lane l owns pixel pairs at tile column 2*(l % ppr),
 // rows l / ppr + RPI*j.  PITCH is the staged pitch, BH the block height.
 // pri_on / sec_on: the tile preset's primary / secondary strength is
 // non-zero; with neither, every sample stays as it is.
@@ -122,7 +170,7 @@ struct DbCdefArgs {
 template <int PITCH, int BH, int RPI, bool EDGE, bool SHIFT>
 __device__ __forceinline__ void filter_pairs(const uint16_t* t, const uint32_t* s1, const DevPlane& d, int px0,
                                              int py0, int tw, const uint8_t* active, const PairBlock* blocks,
-                                             bool pri_on, bool sec_on, int warp, int lane, int sx) {
+                                             bool pri_on, bool sec_on, int br, int lane, int sx) {
     const int ppr = 32 / RPI;              // pairs per row
     const int lp = lane % ppr, lr = lane / ppr;
     const int x = 2 * lp;
@@ -130,7 +178,6 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const uint32_t* 
     const int bx = x >> (3 - sx);
     const int gx = px0 + x;
     const bool col_in = gx < d.width;
-    const int br = warp;                   // 8 block rows, 8 warps
     const int r0 = br * BH;
     if (py0 + r0 >= d.height) return;
     const int rows_here = min(BH, d.height - (py0 + r0));
@@ -183,13 +230,15 @@ template <int PITCH, int BH, int RPI, bool SHIFT>
 __device__ __forceinline__ void filter_pairs_edge(bool edge, const uint16_t* t, const uint32_t* s1, const DevPlane& d,
                                                   int px0, int py0, int tw, const uint8_t* active,
                                                   const PairBlock* blocks, bool pri_on, bool sec_on, int warp,
-                                                  int lane, int sx) {
-    if (edge)
-        filter_pairs<PITCH, BH, RPI, true, SHIFT>(t, s1, d, px0, py0, tw, active, blocks, pri_on, sec_on, warp, lane,
-                                                 sx);
-    else
-        filter_pairs<PITCH, BH, RPI, false, SHIFT>(t, s1, d, px0, py0, tw, active, blocks, pri_on, sec_on, warp, lane,
-                                                  sx);
+                                                  int lane, int sx, int nwarps) {
+    for (int br = warp; br < 8; br += nwarps) {  // 8 block rows
+        if (edge)
+            filter_pairs<PITCH, BH, RPI, true, SHIFT>(t, s1, d, px0, py0, tw, active, blocks, pri_on, sec_on, br, lane,
+                                                     sx);
+        else
+            filter_pairs<PITCH, BH, RPI, false, SHIFT>(t, s1, d, px0, py0, tw, active, blocks, pri_on, sec_on, br,
+                                                      lane, sx);
+    }
 }
 
 // Segment-list entry: level (6 bits) | samples on the q side, capped at 8 (4)
@@ -222,7 +271,7 @@ __device__ __forceinline__ void filter_line_class(int cls, uint16_t* q, int step
 // the lines the window needs: rows [py0-7, py0+th+7) / [py0-3, py0+th+3) in
 // pass 0, columns [px0-2, px0+tw+2) in pass 1.  Within a pass no two edges
 // touch a common sample, so the lines run in place in any order.
-template <int PASS>
+template <int PASS, int NT>
 __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem, int x0, int y0,
                                              const SideWindow& side, uint32_t* s_list, int* s_count) {
     const int tid = threadIdx.x;
@@ -233,7 +282,7 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
     const int nac = PASS == 0 ? gc.th / 4 + 2 : gc.th / 4 + 1, nbc = PASS == 0 ? gc.tw / 4 + 1 : gc.tw / 4 + 2;
     const int n0 = na0 * nb0, nc = a.num_planes > 1 ? nac * nbc : 0;
     const unsigned m0 = small_div_magic(nb0), mc = small_div_magic(nbc);
-    for (int i = tid; i < n0 + 2 * nc; i += kThreads) {
+    for (int i = tid; i < n0 + 2 * nc; i += NT) {
         int p = 0, j = i;
         if (j >= n0) {
             j -= n0;
@@ -288,7 +337,7 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
     __syncthreads();
     const int c0 = s_count[0], c1 = s_count[1], c2 = s_count[2], c3 = s_count[3];
     const int lines = 4 * (c0 + c1 + c2 + c3);
-    for (int item = tid; item < lines; item += kThreads) {
+    for (int item = tid; item < lines; item += NT) {
         int seg = item >> 2, cls = 0;
         const int line = item & 3;
         if (seg >= c0) {
@@ -324,8 +373,11 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
 // One 64x64 filter block (tile_x, tile_y) of one frame.  Every thread of the
 // CTA calls it; it ends with all threads past their last shared-memory use
 // only after the caller's next __syncthreads().
-__device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int tile_y) {
-    extern __shared__ __align__(16) uint16_t smem[];
+template <int NT>
+__device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int tile_y, const DbCdefTma* tma) {
+    constexpr int kWarpsNT = NT / 32;
+    extern __shared__ __align__(128) uint16_t smem[];
+    __shared__ uint64_t s_mbar;
     __shared__ int s_cost[64][8];
     __shared__ PairBlock s_pair[3][64];
     __shared__ uint8_t s_active[64];
@@ -362,18 +414,44 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         s_active[tid] = act;
     }
 
-    // ---- every plane's tile with an 8-sample halo (edge-clamped).  Whole
-    // 16-byte chunks inside the plane go by cp.async, all in flight at once;
-    // chunks that straddle the left/right plane edge are gathered sample by
-    // sample.  Rows past the top/bottom edge repeat the edge row.
-    for (int p = 0; p < a.num_planes; ++p) {
+    // ---- every plane's tile with an 8-sample halo (edge-clamped).  When the
+    // staged region lies inside every plane, one thread stages each plane's
+    // box with a tensor copy (TMA).  Otherwise whole 16-byte chunks inside the
+    // plane go by cp.async, all in flight at once; chunks that straddle the
+    // left/right plane edge are gathered sample by sample, and rows past the
+    // top/bottom edge repeat the edge row.
+    bool tma_tile = tma != nullptr && tma->use;
+    for (int p = 0; p < a.num_planes && tma_tile; ++p) {
+        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+        tma_tile = px0 >= kHalo && py0 >= kHalo && px0 + g.tw + kHalo <= a.src[p].width &&
+                   py0 + g.th + kHalo <= a.src[p].height && (smem_u32(smem + a.plane_off[p]) & 127) == 0;
+    }
+    if (tma_tile) {  // uniform over the CTA
+        if (tid == 0) mbar_init(&s_mbar, 1);
+        __syncthreads();
+        if (tid == 0) {
+            unsigned bytes = 0;
+            for (int p = 0; p < a.num_planes; ++p) {
+                const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+                bytes += (unsigned)(g.pitch * g.rows * 2);
+            }
+            mbar_expect_tx(&s_mbar, bytes);
+            for (int p = 0; p < a.num_planes; ++p) {
+                const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+                tma_load_2d(smem + a.plane_off[p], &tma->map[p], (x0 >> g.sx) - kHalo, (y0 >> g.sy) - kHalo,
+                            &s_mbar);
+            }
+        }
+    }
+    for (int p = 0; p < a.num_planes && !tma_tile; ++p) {
         const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
         const DevPlaneC& P = a.src[p];
         uint16_t* t = smem + a.plane_off[p];
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
         const int vpr = g.pitch / 8;
         const unsigned mv = small_div_magic(vpr);
-        for (int v = tid; v < g.rows * vpr; v += kThreads) {
+        for (int v = tid; v < g.rows * vpr; v += NT) {
             const int r = small_div(v, mv), cv = v - r * vpr;
             const int y = clampi(py0 - kHalo + r, 0, P.height - 1);
             const int x = px0 - kHalo + cv * 8;
@@ -395,7 +473,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     {
         const int crows = (a.mi_rows + a.ssy) >> a.ssy, ccols = (a.mi_cols + a.ssx) >> a.ssx;
         const int cr0 = (mi_r0 >> a.ssy) - kWinTop, cc0 = (mi_c0 >> a.ssx) - kWinLeft;
-        for (int i = tid; i < kWinCells; i += kThreads) {
+        for (int i = tid; i < kWinCells; i += NT) {
             const int wr = i / kWinCols, wc = i - wr * kWinCols;
             const int r = mi_r0 - kWinTop + wr, c = mi_c0 - kWinLeft + wc;
             if (r >= 0 && c >= 0 && r < a.mi_rows && c < a.mi_cols) {
@@ -407,14 +485,25 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
                 s_side.tx[1][i] = __ldg(a.tx_chroma + (long)(cr0 + wr) * ccols + cc0 + wc);
         }
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (tma_tile) {
+        bool done = false;
+        for (int it = 0; it < kTmaWaitIters && !done; ++it) done = mbar_try_wait(&s_mbar, 0);
+        if (!done) {
+            // The copies never completed: fail the frame, then wait once more
+            // (bounded) so no copy is left writing this CTA's shared memory.
+            report_error(a.status, STAGE_DEBLOCK, 0, VACO_AV1_MSG_TIMEOUT);
+            for (int it = 0; it < kTmaWaitIters && !done; ++it) done = mbar_try_wait(&s_mbar, 0);
+        }
+    } else {
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+    }
     const bool any_active = __syncthreads_or(act);
 
     // ---- input checks from shared memory: the tile's own cells (transform
     // sizes, levels) and the tile's own samples
     {
         int bad = 0;
-        for (int i = tid; i < 256; i += kThreads) {
+        for (int i = tid; i < 256; i += NT) {
             const int r = mi_r0 + (i >> 4), c = mi_c0 + (i & 15);
             if (r < a.mi_rows && c < a.mi_cols) {
                 const int w = (i >> 4) + kWinTop, wc = (i & 15) + kWinLeft;
@@ -428,7 +517,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         if (a.num_planes > 1) {
             const int ccols = (a.mi_cols + a.ssx) >> a.ssx, crows = (a.mi_rows + a.ssy) >> a.ssy;
             const int cw = 16 >> a.ssx, ch = 16 >> a.ssy;
-            for (int i = tid; i < cw * ch; i += kThreads) {
+            for (int i = tid; i < cw * ch; i += NT) {
                 const int dr = i >> (4 - a.ssx), dc = i - dr * cw;  // cw = 16 >> ssx
                 const int r = (mi_r0 >> a.ssy) + dr, c = (mi_c0 >> a.ssx) + dc;
                 if (r < crows && c < ccols) bad |= s_side.tx[1][(dr + kWinTop) * kWinCols + dc + kWinLeft] > 18;
@@ -445,7 +534,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
             const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
             const int cpr = g.tw / 8, rows = min(g.th, P.height - py0);
             const uint16_t* t = smem + a.plane_off[p];
-            for (int v = tid; v < rows * cpr; v += kThreads) {
+            for (int v = tid; v < rows * cpr; v += NT) {
                 const int r = v >> (3 - g.sx), cv = v - r * cpr;  // cpr = tw / 8 = 8 >> sx
                 const int x = px0 + cv * 8;
                 if (x >= P.width) continue;
@@ -463,8 +552,8 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
 
     // ---- deblocking, pass 0 (vertical edges) then pass 1 (horizontal edges)
     if (a.deblock_on) {
-        deblock_pass<0>(a, smem, x0, y0, s_side, s_list, s_count);
-        deblock_pass<1>(a, smem, x0, y0, s_side, s_list, s_count);
+        deblock_pass<0, NT>(a, smem, x0, y0, s_side, s_list, s_count);
+        deblock_pass<1, NT>(a, smem, x0, y0, s_side, s_list, s_count);
     }
 
     // ---- stripe-boundary rows of the deblocked picture for restoration:
@@ -481,7 +570,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         // the tile (th rows, th a multiple of the stripe height or half of it)
         // holds boundary rows y = k*sh - off - 2 + sub, sub < 4
         const int lsh = 6 - g.sy;  // log2 of the stripe height
-        for (int i = warp; i < 4 * ((g.th >> lsh) + 1); i += kThreads / 32) {
+        for (int i = warp; i < 4 * ((g.th >> lsh) + 1); i += kWarpsNT) {
             const int kk = i >> 2, sub = i & 3;
             const int kb = ((py0 + off + 2) >> lsh) + kk;
             const int y = kb * sh - off - 2 + sub;
@@ -500,7 +589,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
             const DevPlane& d = a.dst[p];
             const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
             const uint16_t* t = smem + a.plane_off[p];
-            for (int r = warp; r < g.th; r += kThreads / 32) {
+            for (int r = warp; r < g.th; r += kWarpsNT) {
                 const int y = py0 + r;
                 if (y >= d.height) break;
                 for (int c = lane; c < g.tw; c += 32)
@@ -518,7 +607,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         uint16_t* t = smem + a.plane_off[p];
         const int wr = g.th + 4, wc = g.tw + 4;
         const unsigned mw = small_div_magic(wc);
-        for (int i = tid; i < wr * wc; i += kThreads) {
+        for (int i = tid; i < wr * wc; i += NT) {
             const int r = small_div(i, mw), c = i - r * wc;
             const int y = py0 - 2 + r, x = px0 - 2 + c;
             if (y < 0 || x < 0 || y >= d.height || x >= d.width)
@@ -534,18 +623,18 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     {
         constexpr int WP = (64 + 2 * kHalo) / 2, W0 = (kHalo - 1) / 2, NW = 64 / 2 + 1;
         const uint32_t* t32 = reinterpret_cast<const uint32_t*>(smem + a.plane_off[0]);
-        for (int i = tid; i < kShiftRows * NW; i += kThreads) {
+        for (int i = tid; i < kShiftRows * NW; i += NT) {
             const int r = i / NW, w = W0 + (i - r * NW);
             const int src = (kHalo - 2 + r) * WP + w;
             s_u.shifted[r * WP + w] = __byte_perm(t32[src], t32[src + 1], 0x5432);
         }
     }
 
-    // Direction search: warp w handles direction pair (w & 3) for blocks
-    // (w >> 2)*32 + lane (warp-uniform branches).
+    // Direction search: job j (0..7, spread over the warps) handles direction
+    // pair (j & 3) for blocks (j >> 2)*32 + lane (warp-uniform branches).
     const int lpitch = 64 + 2 * kHalo;
-    {
-        const int pair = warp & 3, b = ((warp >> 2) << 5) + lane;
+    for (int job = warp; job < 8; job += kWarpsNT) {
+        const int pair = job & 3, b = ((job >> 2) << 5) + lane;
         if (s_active[b]) {
             const uint16_t* blk = smem + a.plane_off[0] + (kHalo + (b >> 3) * 8) * lpitch + kHalo + (b & 7) * 8;
             int lo, hi;
@@ -556,8 +645,9 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     }
     __syncthreads();
     // Per block and plane (one thread each): direction, strengths, checks.
-    if (tid < 64 * a.num_planes && s_active[tid & 63]) {
-        const int b = tid & 63, p = tid >> 6;
+    for (int i = tid; i < 64 * a.num_planes; i += NT) {
+        if (!s_active[i & 63]) continue;
+        const int b = i & 63, p = i >> 6;
         int dir;
         uint32_t var;
         best_direction(s_cost[b], dir, var);
@@ -601,34 +691,40 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         // tile layouts: 64x64 (luma, 4:4:4 chroma), 32x32 (4:2:0), 32x64 (4:2:2)
         if (p == 0) {
             filter_pairs_edge<64 + 2 * kHalo, 8, 1, true>(edge, tp, s_u.shifted, d, px0, py0, g.tw, s_active,
-                                                          s_pair[p], pri_on, sec_on, warp, lane, g.sx);
+                                                          s_pair[p], pri_on, sec_on, warp, lane, g.sx, kWarpsNT);
         } else if (g.tw == 64) {
             filter_pairs_edge<64 + 2 * kHalo, 8, 1, false>(edge, tp, nullptr, d, px0, py0, g.tw, s_active, s_pair[p],
-                                                           pri_on, sec_on, warp, lane, g.sx);
+                                                           pri_on, sec_on, warp, lane, g.sx, kWarpsNT);
         } else if (g.th == 32) {
             filter_pairs_edge<32 + 2 * kHalo, 4, 2, false>(edge, tp, nullptr, d, px0, py0, g.tw, s_active, s_pair[p],
-                                                           pri_on, sec_on, warp, lane, g.sx);
+                                                           pri_on, sec_on, warp, lane, g.sx, kWarpsNT);
         } else {
             filter_pairs_edge<32 + 2 * kHalo, 8, 2, false>(edge, tp, nullptr, d, px0, py0, g.tw, s_active, s_pair[p],
-                                                           pri_on, sec_on, warp, lane, g.sx);
+                                                           pri_on, sec_on, warp, lane, g.sx, kWarpsNT);
         }
     }
 }
 
-// MIN_CTAS CTAs per SM: 3 leaves 80 registers a thread (fewer instructions
-// and instruction-fetch stalls, 1 % faster on a 4K frame); 4 fills more SMs
-// at once, which wins when a frame has few tiles (a 1080p frame's 510 tiles
-// fit one wave of 4 per SM; at 3 per SM they take two).
-template <int MIN_CTAS>
-__global__ void __launch_bounds__(kThreads, MIN_CTAS) dbcdef_kernel(DbCdefArgs a) {
-    dbcdef_tile(a, blockIdx.x, blockIdx.y);
+// NT threads per tile, MIN_CTAS CTAs per SM.  With 256 threads, 3 CTAs
+// leave 80 registers a thread (fewer instructions and instruction-fetch
+// stalls, 1 % faster on a 4K frame) and 4 fill more SMs at once, which wins
+// when a frame has few tiles (a 1080p frame's 510 tiles fit one wave of 4 per
+// SM; at 3 per SM they take two).  128 threads at 5 CTAs per SM is the
+// smaller-CTA shape: shorter barriers, about the same warps per SM.
+template <int NT, int MIN_CTAS>
+__global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_kernel(DbCdefArgs a, const __grid_constant__ DbCdefTma tma) {
+    overlap_prologue();
+    dbcdef_tile<NT>(a, blockIdx.x, blockIdx.y, &tma);
 }
 
 // Persistent form: CTAs take tiles of all frames of a batch from a device
 // queue (one atomic per tile), so frames of any size share one launch.
-__global__ void __launch_bounds__(kThreads, 4) dbcdef_batch_kernel(const DbCdefArgs* __restrict__ frames,
-                                                                   const int* __restrict__ tile_prefix, int n,
-                                                                   int* queue) {
+// MIN_CTAS as for dbcdef_kernel: the launch picks the body whose register
+// budget matches the persistent grid's CTAs per SM.
+template <int NT, int MIN_CTAS>
+__global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_batch_kernel(const DbCdefArgs* __restrict__ frames,
+                                                                    const int* __restrict__ tile_prefix, int n,
+                                                                    int* queue) {
     __shared__ int s_tile, s_frame;
     __shared__ DbCdefArgs s_args;
     const int total = tile_prefix[n];
@@ -652,12 +748,12 @@ __global__ void __launch_bounds__(kThreads, 4) dbcdef_batch_kernel(const DbCdefA
             const int words = (int)(sizeof(DbCdefArgs) / sizeof(int));
             const int* src = reinterpret_cast<const int*>(frames + f);
             int* dst = reinterpret_cast<int*>(&s_args);
-            for (int i = threadIdx.x; i < words; i += kThreads) dst[i] = src[i];
+            for (int i = threadIdx.x; i < words; i += NT) dst[i] = src[i];
         }
         __syncthreads();
         const int local = t - tile_prefix[f];
         const int tiles_x = (s_args.mi_cols + 15) / 16;
-        dbcdef_tile(s_args, local % tiles_x, local / tiles_x);
+        dbcdef_tile<NT>(s_args, local % tiles_x, local / tiles_x, nullptr);
     }
 }
 
@@ -729,25 +825,74 @@ cudaError_t dbcdef_kernel_attributes() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && !(g_attr_devices.load(std::memory_order_acquire) & (1ull << dev))) {
-        cudaError_t e = cudaFuncSetAttribute(dbcdef_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(dbcdef_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(dbcdef_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        constexpr int kMaxSmem = 96 * 1024;
+        const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+        cudaError_t e = cudaFuncSetAttribute(dbcdef_kernel<256, 3>, attr, kMaxSmem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_kernel<256, 4>, attr, kMaxSmem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_kernel<128, 5>, attr, kMaxSmem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<256, 3>, attr, kMaxSmem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<256, 4>, attr, kMaxSmem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<128, 5>, attr, kMaxSmem);
         if (e != cudaSuccess) return e;
         g_attr_devices.fetch_or(1ull << dev, std::memory_order_release);
     }
     return cudaSuccess;
 }
 
+namespace {
+
+// cuTensorMapEncodeTiled from the driver, resolved once through the runtime
+// (no link against the driver library); null when unavailable.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::atomic<void*> fn{nullptr};
+    static std::atomic<int> tried{0};
+    void* f = fn.load(std::memory_order_acquire);
+    if (f || tried.load(std::memory_order_acquire)) return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess && p)
+        fn.store(p, std::memory_order_release);
+    tried.store(1, std::memory_order_release);
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn.load(std::memory_order_acquire));
+}
+
+// Tensor maps over the frame's input planes with the staged box of each
+// plane (pitch x rows of the tile plus its halo); use = 0 when the planes
+// cannot be described (alignment) or the encoder is unavailable.
+void build_tma(const DbCdefArgs& a, DbCdefTma* t) {
+    memset(t, 0, sizeof *t);
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode || !a.vec_ok) return;  // vec_ok: 16-byte base and a stride of whole 16-byte units
+    for (int p = 0; p < a.num_planes; ++p) {
+        const int sx = p ? a.ssx : 0, sy = p ? a.ssy : 0;
+        const cuuint64_t dims[2] = {(cuuint64_t)a.src[p].width, (cuuint64_t)a.src[p].height};
+        const cuuint64_t strides[1] = {(cuuint64_t)a.src[p].stride * 2};
+        const cuuint32_t box[2] = {(cuuint32_t)((64 >> sx) + 2 * kHalo), (cuuint32_t)((64 >> sy) + 2 * kHalo)};
+        const cuuint32_t elem[2] = {1, 1};
+        if (a.src[p].width <= 0 || a.src[p].height <= 0 ||
+            encode(&t->map[p], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<uint16_t*>(a.src[p].data), dims, strides,
+                   box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return;
+    }
+    t->use = 1;
+}
+
+}  // namespace
+
 cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
     DbCdefArgs a;
     const size_t smem = build_dbcdef_args(L, &a);
+    DbCdefTma tma;
+    build_tma(a, &tma);
     cudaError_t e = dbcdef_kernel_attributes();
     if (e != cudaSuccess) return e;
     dim3 grid(div_up(L.info.mi_cols, 16), div_up(L.info.mi_rows, 16));
-    // 3 CTAs per SM once the frame has more than 2.5 waves of 4 per SM
-    // (measured best on 4K and 2880-wide frames; 4 on 1080p and 2560-wide).
+    if (L.threads == 128) return launch_overlapped(dbcdef_kernel<128, 5>, grid, dim3(128), smem, stream, a, tma);
+    // 256 threads: 3 CTAs per SM once the frame has more than 2.5 waves of 4
+    // per SM (measured best on 4K and 2880-wide frames; 4 on 1080p and
+    // 2560-wide).
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64) {
@@ -757,18 +902,21 @@ cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
         if (n > 0) sms = n;
     }
     if ((long)grid.x * grid.y * 2 > 5L * 4 * sms)
-        dbcdef_kernel<3><<<grid, kThreads, smem, stream>>>(a);
-    else
-        dbcdef_kernel<4><<<grid, kThreads, smem, stream>>>(a);
-    return cudaGetLastError();
+        return launch_overlapped(dbcdef_kernel<256, 3>, grid, dim3(256), smem, stream, a, tma);
+    return launch_overlapped(dbcdef_kernel<256, 4>, grid, dim3(256), smem, stream, a, tma);
 }
 
 cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, size_t smem,
-                                int grid, cudaStream_t stream) {
+                                int grid, int ctas_per_sm, int threads, cudaStream_t stream) {
     cudaError_t e = dbcdef_kernel_attributes();
     if (e != cudaSuccess) return e;
-    dbcdef_batch_kernel<<<grid, kThreads, smem, stream>>>(static_cast<const DbCdefArgs*>(dev_args), dev_prefix, n,
-                                                         dev_queue);
+    const DbCdefArgs* args = static_cast<const DbCdefArgs*>(dev_args);
+    if (threads == 128)
+        dbcdef_batch_kernel<128, 5><<<grid, 128, smem, stream>>>(args, dev_prefix, n, dev_queue);
+    else if (ctas_per_sm <= 3)  // up to 3 resident: the 80-register body
+        dbcdef_batch_kernel<256, 3><<<grid, 256, smem, stream>>>(args, dev_prefix, n, dev_queue);
+    else
+        dbcdef_batch_kernel<256, 4><<<grid, 256, smem, stream>>>(args, dev_prefix, n, dev_queue);
     return cudaGetLastError();
 }
 

@@ -146,16 +146,19 @@ struct DbCdefLaunch {
     int cdef_stride, cdef_count;
     vaco_av1_cdef_params cdef;
     DeviceStatus* status;
+    int threads = 256;          // threads per tile: 256 or 128
 };
 cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream);
 // Batched form: `dev_args` holds n per-frame argument records (dbcdef_args_size()
 // bytes each, built by build_dbcdef_args), `dev_prefix` n+1 running tile
-// counts, `dev_queue` a zeroed counter.  `grid` persistent CTAs drain the queue.
+// counts, `dev_queue` a zeroed counter.  `grid` persistent CTAs drain the queue;
+// `ctas_per_sm` (grid / SMs) and `threads` (per tile, 256 or 128) pick the
+// kernel body compiled for that shape.
 size_t dbcdef_args_size();
 size_t build_dbcdef_args(const DbCdefLaunch& L, void* out);  // returns dynamic smem bytes
 inline int dbcdef_tiles(const vaco_av1_frame_info& i) { return ((i.mi_cols + 15) / 16) * ((i.mi_rows + 15) / 16); }
 cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, size_t smem,
-                                int grid, cudaStream_t stream);
+                                int grid, int ctas_per_sm, int threads, cudaStream_t stream);
 // Rows in the compact boundary buffer of a plane of `height` rows.
 inline int pre_rows_count(int height, int sub_y) {
     const int sh = 64 >> sub_y, off = 8 >> sub_y;

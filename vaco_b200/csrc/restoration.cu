@@ -559,7 +559,10 @@ __device__ __forceinline__ void lr_tile(const LrArgs& a, int block) {
     }
 }
 
-__global__ void __launch_bounds__(kLrThreads, 4) restoration_kernel(LrArgs a) { lr_tile(a, blockIdx.x); }
+__global__ void __launch_bounds__(kLrThreads, 4) restoration_kernel(LrArgs a) {
+    overlap_prologue();
+    lr_tile(a, blockIdx.x);
+}
 
 // Persistent form over the tiles of all frames of a batch (see dbcdef.cu).
 __global__ void __launch_bounds__(kLrThreads, 4) restoration_batch_kernel(const LrArgs* __restrict__ frames,
@@ -691,8 +694,8 @@ cudaError_t launch_restoration(const LrPlane* planes, int count, int bit_depth, 
     const int total = build_lr_args(planes, count, bit_depth, &a);
     cudaError_t e = lr_kernel_attributes();
     if (e != cudaSuccess) return e;
-    if (total > 0) restoration_kernel<<<total, kLrThreads, kLrSmem, stream>>>(a);
-    return cudaGetLastError();
+    if (total == 0) return cudaSuccess;
+    return launch_overlapped(restoration_kernel, dim3(total), dim3(kLrThreads), kLrSmem, stream, a);
 }
 
 cudaError_t launch_restoration_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, int grid,

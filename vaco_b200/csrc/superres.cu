@@ -107,6 +107,7 @@ struct SrArgs {
 // CTAs whose staged span holds such a sample.
 __global__ void __launch_bounds__(kSrThreads) superres_kernel(SrArgs a) {
     __shared__ uint4 s_col[kSrMaxSpan][kSrGroups];
+    overlap_prologue();
     const int blk_all = blockIdx.x;
     int k = 0;
     while (k + 1 < a.count && blk_all >= a.p[k + 1].first_block) ++k;
@@ -242,8 +243,7 @@ cudaError_t launch_superres(const SuperresPlane* planes, int count, int bit_dept
     a.status = status;
     a.stage = stage;
     if (blocks == 0) return cudaSuccess;  // nothing to upscale
-    superres_kernel<<<(unsigned)blocks, kSrThreads, 0, stream>>>(a);
-    return cudaGetLastError();
+    return launch_overlapped(superres_kernel, dim3((unsigned)blocks), dim3(kSrThreads), 0, stream, a);
 }
 
 }  // namespace vaco

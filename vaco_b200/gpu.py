@@ -241,10 +241,12 @@ class Context:
         lib().vaco_av1_ctx_get_tuning(self.handle, C.byref(t))
         return t
 
-    def set_tuning(self, dbcdef_ctas_per_sm=None, lr_ctas_per_sm=None, use_graphs=None, largest_first=None):
+    def set_tuning(self, dbcdef_ctas_per_sm=None, lr_ctas_per_sm=None, use_graphs=None, largest_first=None,
+                   dbcdef_threads=None):
         t = self.tuning
         for name, v in (("dbcdef_ctas_per_sm", dbcdef_ctas_per_sm), ("lr_ctas_per_sm", lr_ctas_per_sm),
-                        ("use_graphs", use_graphs), ("largest_first", largest_first)):
+                        ("use_graphs", use_graphs), ("largest_first", largest_first),
+                        ("dbcdef_threads", dbcdef_threads)):
             if v is not None:
                 setattr(t, name, int(v))
         st = lib().vaco_av1_ctx_set_tuning(self.handle, C.byref(t))
