@@ -662,8 +662,9 @@ VACO_AV1_API int32_t vaco_av1_film_grain_host(vaco_av1_ctx* ctx, const vaco_av1_
  * kernel of vaco_av1_postfilter_frame_dev), with identical output.
  * All calls share the array.  Calls whose GPU work overlaps race and produce
  * undefined output.
- * The first call on a device resolves the array's address on that device;
- * make it before any stream capture begins there.
+ * The first call on a device does a one-time set-up there: it looks up the
+ * array's device address (cudaGetSymbolAddress) and caches it.  Make that
+ * first call before any stream capture begins on the device.
  * Works on the current device and synchronizes `stream` once. */
 VACO_AV1_API int32_t vaco_av1_postfilter_frame_noalloc(void* stream, const vaco_av1_frame_job* job,
                                                        int32_t* msg);

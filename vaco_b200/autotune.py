@@ -1,9 +1,14 @@
-"""Launch-shape autotuner for the batched form.
+"""Launch-shape autotuner for the batched form and the per-frame chain.
 
-Sweeps the persistent grid of both per-stage kernels (CTAs per SM), CUDA-graph
-replay and the tile-queue order on the batch workload (64 mixed frames) with
-CUDA-event timing, and writes the fastest setting to tuned/<gpu>.json, which
-load_tuning() reads.  Run on the target GPU:
+Sweeps, with CUDA-event timing on the target GPU:
+  batch  (64 mixed frames, config 3): threads per 64x64 tile of the fused
+         deblock+CDEF kernel (256 or 128) with its persistent CTAs per SM,
+         the restoration kernel's persistent CTAs per SM, CUDA-graph replay
+         and the tile-queue order;
+  frame  (4K 10-bit frames back to back): threads per tile of the fused
+         kernel on the per-frame path.
+and writes the fastest settings to tuned/<gpu>.json, which load_tuning()
+reads.  Run on the target GPU:
 
     python -m vaco_b200.autotune
 """
@@ -41,7 +46,29 @@ def load_tuning() -> dict:
     return dict(DEFAULT)
 
 
+# (threads per tile, persistent CTAs per SM) of the fused kernel: 256-thread
+# tiles at 2-4 per SM, 128-thread tiles at 4-6 (about the same warps per SM)
+DBCDEF_SHAPES = ((256, 2), (256, 3), (256, 4), (128, 4), (128, 5), (128, 6))
+
+
+def _time(fn, reps, stream):
+    import torch
+
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
 def main(argv=None):
+    import itertools
+
     import torch
 
     from vaco_b200 import synth
@@ -56,29 +83,42 @@ def main(argv=None):
     jobs = ctx.batch_jobs(devs)
     stream = torch.cuda.current_stream()
     results = []
-    for db, lr, graphs, largest in itertools.product((2, 3, 4), (2, 3, 4), (0, 1), (0, 1)):
-        ctx.set_tuning(dbcdef_ctas_per_sm=db, lr_ctas_per_sm=lr, use_graphs=graphs, largest_first=largest)
-        for _ in range(3):
-            ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(10):
-            ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / 10
-        cfg = {"dbcdef_ctas_per_sm": db, "lr_ctas_per_sm": lr, "use_graphs": graphs, "largest_first": largest}
+    for (threads, db), lr, graphs, largest in itertools.product(DBCDEF_SHAPES, (3, 4), (0, 1), (0, 1)):
+        cfg = {"dbcdef_threads": threads, "dbcdef_ctas_per_sm": db, "lr_ctas_per_sm": lr, "use_graphs": graphs,
+               "largest_first": largest}
+        ctx.set_tuning(**cfg)
+        ms = _time(lambda: ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs), 10, stream)
         results.append((ms, cfg))
         print(json.dumps({"ms_per_batch": round(ms, 4), **cfg}), flush=True)
     results.sort(key=lambda r: r[0])
     best_ms, best = results[0]
+    del devs, jobs
+    # per-frame chain: 4K 10-bit frames back to back (deferred status)
+    k4 = [DeviceFrame(synth.make_frame(synth.CONFIG1, synth.seed_for(3, 6000 + i))) for i in range(8)]
+    ctx.set_deferred_status(True)
+    frame_results = []
+    for threads in (256, 128):
+        ctx.set_tuning(dbcdef_threads=threads)
+
+        def run():
+            for d in k4:
+                ctx.postfilter_frame_dev(d, stream.cuda_stream)
+
+        ms = _time(run, 50, stream) / len(k4)
+        ctx.flush(stream.cuda_stream)
+        frame_results.append((ms, {"dbcdef_threads": threads}))
+        print(json.dumps({"frame_ms": round(ms, 5), "dbcdef_threads": threads}), flush=True)
+    ctx.set_deferred_status(False)
+    frame_results.sort(key=lambda r: r[0])
     out = {"gpu": torch.cuda.get_device_name(0), "workload": "64 mixed frames (synthetic batch mix)",
            "batch": best, "ms_per_batch": round(best_ms, 4),
-           "sweep": [{"ms_per_batch": round(m, 4), **c} for m, c in results]}
+           "frame": dict(frame_results[0][1], ms_per_4k_frame=round(frame_results[0][0], 5)),
+           "sweep": [{"ms_per_batch": round(m, 4), **c} for m, c in results],
+           "frame_sweep": [{"ms_per_4k_frame": round(m, 5), **c} for m, c in frame_results]}
     TUNED.mkdir(exist_ok=True)
     path = pathlib.Path(argv[0]) if argv else TUNED / f"{gpu_key()}.json"
     path.write_text(json.dumps(out, indent=1) + "\n")
-    print(f"best {best} at {best_ms:.4f} ms/batch -> {path}")
+    print(f"best {best} at {best_ms:.4f} ms/batch; per frame {frame_results[0][1]} -> {path}")
     ctx.close()
 
 
