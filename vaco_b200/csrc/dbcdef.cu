@@ -42,7 +42,6 @@ namespace {
 using namespace cdefk;
 using namespace dbk;
 
-constexpr int kThreads = 256;
 constexpr int kHalo = 8;
 // Edge segments (one edge x one 4-sample cell) per pass and plane are at most
 // (th/4+4) x (tw/4+1) = 340.  Size-class lists: 0 = size 4 (any plane, up to
