@@ -225,6 +225,7 @@ pub struct Tuning {
     pub use_graphs: i32,
     pub largest_first: i32,
     pub dbcdef_threads: i32,
+    pub stage_fusion: i32,
 }
 
 #[repr(C)]

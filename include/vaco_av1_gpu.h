@@ -409,6 +409,9 @@ typedef struct vaco_av1_tuning {
     int32_t dbcdef_threads;      /* threads per 64x64 tile of the deblock+CDEF kernel, in the
                                     batched form and vaco_av1_postfilter_frame_dev: 256 or
                                     128 (0 = 256) */
+    int32_t stage_fusion;        /* batched form: 1 = deblocking and CDEF in one fused
+                                    kernel; 0 = as separate per-stage kernels, frame by
+                                    frame */
 } vaco_av1_tuning;
 
 VACO_AV1_API int32_t vaco_av1_ctx_set_tuning(vaco_av1_ctx* ctx, const vaco_av1_tuning* tuning);

@@ -88,3 +88,38 @@ def test_config3_full_mix_matches_oracle(ctx, oracle_threads):
         assert m == 0
         for k, (g, w) in enumerate(zip(d.outputs_numpy(), want)):
             assert np.array_equal(g, w), f"frame {i} ({f.coded_width}x{f.coded_height}) plane {k} differs"
+
+
+@pytest.mark.parametrize("shape", [(256, 3, 1), (128, 5, 1), (256, 4, 0)], ids=["fused256", "fused128", "unfused"])
+def test_batch_launch_shapes_and_stage_fusion_match_oracle(ctx, shape, oracle_threads):
+    """Every launch shape and stage-fusion choice the autotuner may pick gives
+    the oracle's planes (superres frames and restoration included)."""
+    threads, ctas, fusion = shape
+    ctx.set_tuning(dbcdef_threads=threads, dbcdef_ctas_per_sm=ctas, stage_fusion=fusion, use_graphs=1)
+    try:
+        frames = mixed_frames(900)
+        devs = [DeviceFrame(f) for f in frames]
+        st, ms = ctx.postfilter_batch_dev(devs, stream=torch.cuda.current_stream().cuda_stream)
+        assert st == [0] * len(frames) and ms == [0] * len(frames)
+        for f, d in zip(frames, devs):
+            want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+            assert m == 0
+            for g, w in zip(d.outputs_numpy(), want):
+                np.testing.assert_array_equal(g, w)
+    finally:
+        ctx.set_tuning(dbcdef_threads=256, dbcdef_ctas_per_sm=3, stage_fusion=1)
+
+
+def test_per_frame_128_thread_tiles_match_oracle(ctx, oracle_threads):
+    """The per-frame chain with 128-thread tiles of the fused kernel."""
+    ctx.set_tuning(dbcdef_threads=128)
+    try:
+        for f in mixed_frames(950, small=False):
+            want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+            assert m == 0
+            d = DeviceFrame(f)
+            ctx.postfilter_frame_dev(d)
+            for g, w in zip(d.outputs_numpy(), want):
+                np.testing.assert_array_equal(g, w)
+    finally:
+        ctx.set_tuning(dbcdef_threads=256)

@@ -177,6 +177,7 @@ class Tuning(C.Structure):
         ("use_graphs", C.c_int32),
         ("largest_first", C.c_int32),
         ("dbcdef_threads", C.c_int32),
+        ("stage_fusion", C.c_int32),
     ]
 
 

@@ -3,8 +3,9 @@
 Sweeps, with CUDA-event timing on the target GPU:
   batch  (64 mixed frames, config 3): threads per 64x64 tile of the fused
          deblock+CDEF kernel (256 or 128) with its persistent CTAs per SM,
-         the restoration kernel's persistent CTAs per SM, CUDA-graph replay
-         and the tile-queue order;
+         the restoration kernel's persistent CTAs per SM, CUDA-graph replay,
+         the tile-queue order, and the stage fusion (deblocking and CDEF in
+         one kernel, or as separate kernels);
   frame  (4K 10-bit frames back to back): threads per tile of the fused
          kernel on the per-frame path.
 and writes the fastest settings to tuned/<gpu>.json, which load_tuning()
@@ -21,7 +22,8 @@ import sys
 
 ROOT = pathlib.Path(__file__).resolve().parent.parent
 TUNED = ROOT / "tuned"
-DEFAULT = {"dbcdef_ctas_per_sm": 3, "lr_ctas_per_sm": 4, "use_graphs": 1, "largest_first": 1, "dbcdef_threads": 256}
+DEFAULT = {"dbcdef_ctas_per_sm": 3, "lr_ctas_per_sm": 4, "use_graphs": 1, "largest_first": 1, "dbcdef_threads": 256,
+           "stage_fusion": 1}
 
 
 def gpu_key() -> str:
@@ -90,8 +92,17 @@ def main(argv=None):
         ms = _time(lambda: ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs), 10, stream)
         results.append((ms, cfg))
         print(json.dumps({"ms_per_batch": round(ms, 4), **cfg}), flush=True)
+    # stage fusion: deblocking and CDEF as separate kernels, at the best shape so far
+    results.sort(key=lambda r: r[0])
+    unfused = dict(results[0][1], stage_fusion=0)
+    ctx.set_tuning(**unfused)
+    ms = _time(lambda: ctx.postfilter_batch_dev(devs, stream=stream.cuda_stream, jobs=jobs), 10, stream)
+    results.append((ms, unfused))
+    print(json.dumps({"ms_per_batch": round(ms, 4), **unfused}), flush=True)
+    ctx.set_tuning(stage_fusion=1)
     results.sort(key=lambda r: r[0])
     best_ms, best = results[0]
+    best = dict(best, stage_fusion=best.get("stage_fusion", 1))
     del devs, jobs
     # per-frame chain: 4K 10-bit frames back to back (deferred status)
     k4 = [DeviceFrame(synth.make_frame(synth.CONFIG1, synth.seed_for(3, 6000 + i))) for i in range(8)]

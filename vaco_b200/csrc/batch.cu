@@ -68,6 +68,7 @@ struct FramePlan {
     bool run_db = false, run_lr = false, superres = false, lr_active = false;
     unsigned long long host_key = kNoError;
     PlaneBuf cdef[3], rows[3], ucdef[3], urows[3];
+    PlaneBuf deb[3], udeb[3];  // unfused stages: the whole deblocked picture (and its upscaled copy)
     int np = 0, tiles_db = 0;
     long long pixels = 0;
 };
@@ -101,12 +102,85 @@ int32_t fail(vaco_av1_ctx* ctx, cudaError_t e, int32_t* statuses, int32_t* msgs,
     return VACO_AV1_DEVICE_ERROR;
 }
 
+// Deblocking and CDEF of one frame as separate kernels (the unfused stage
+// choice): copy with checks into the frame's deblocked picture, both passes
+// in place, then CDEF into its CDEF picture (a copy when CDEF is off, as
+// apply_cdef leaves the picture alone).
+cudaError_t enqueue_unfused(const vaco_av1_frame_job& J, const FramePlan& F, unsigned char* base, DeviceStatus* status,
+                            cudaStream_t s) {
+    const vaco_av1_frame_info& info = J.info;
+    const int ssx = info.subsampling_x, ssy = info.subsampling_y;
+    DevPlaneC sp[3];
+    DevPlane deb[3];
+    for (int k = 0; k < F.np; ++k) {
+        sp[k] = DevPlaneC{J.src.planes[k], J.src.width[k], J.src.height[k], J.src.stride[k]};
+        deb[k] = dev_plane(base, F.deb[k]);
+    }
+    const long n_luma = (long)info.mi_rows * info.mi_cols;
+    const long n_chroma = F.np > 1 ? (long)((info.mi_rows + ssy) >> ssy) * ((info.mi_cols + ssx) >> ssx) : 0;
+    cudaError_t e = launch_deblock_prepare(sp, deb, F.np, info.bit_depth, J.tx_luma, n_luma, J.tx_chroma, n_chroma,
+                                           J.lvl_map, status, s);
+    if (e != cudaSuccess) return e;
+    DeblockLaunch L;
+    for (int k = 0; k < 3; ++k) L.pic[k] = k < F.np ? deb[k] : DevPlane{nullptr, 0, 0, 0};
+    L.num_planes = F.np;
+    L.ssx = ssx;
+    L.ssy = ssy;
+    L.bit_depth = info.bit_depth;
+    L.mi_rows = info.mi_rows;
+    L.mi_cols = info.mi_cols;
+    L.coded_width = info.coded_width;
+    L.coded_height = info.coded_height;
+    L.tx_luma = J.tx_luma;
+    L.tx_chroma = J.tx_chroma;
+    L.lvl_map = J.lvl_map;
+    for (int k = 0; k < 4; ++k) L.levels[k] = J.deblock.levels[k];
+    L.sharpness = J.deblock.sharpness;
+    e = launch_deblock_passes(L, s);
+    if (e != cudaSuccess) return e;
+    vaco_av1_picture deb_pic{}, cdef_pic{};
+    for (int k = 0; k < F.np; ++k) {
+        const DevPlane c = dev_plane(base, F.cdef[k]);
+        deb_pic.planes[k] = deb[k].data;
+        deb_pic.width[k] = deb[k].width;
+        deb_pic.height[k] = deb[k].height;
+        deb_pic.stride[k] = deb[k].stride;
+        cdef_pic.planes[k] = c.data;
+        cdef_pic.width[k] = c.width;
+        cdef_pic.height[k] = c.height;
+        cdef_pic.stride[k] = c.stride;
+    }
+    bool all_zero = true;
+    for (int k = 0; k < 8; ++k)
+        all_zero = all_zero && J.cdef.y_primary[k] == 0 && J.cdef.y_secondary[k] == 0 && J.cdef.uv_primary[k] == 0 &&
+                   J.cdef.uv_secondary[k] == 0;
+    if (!J.cdef.enabled || all_zero) {
+        for (int k = 0; k < F.np && e == cudaSuccess; ++k)
+            e = cudaMemcpy2DAsync(cdef_pic.planes[k], (size_t)cdef_pic.stride[k] * 2, deb_pic.planes[k],
+                                  (size_t)deb_pic.stride[k] * 2, (size_t)deb_pic.width[k] * 2, deb_pic.height[k],
+                                  cudaMemcpyDeviceToDevice, s);
+        return e;
+    }
+    CdefLaunch C;
+    C.src = deb_pic;
+    C.dst = cdef_pic;
+    C.info = info;
+    C.skip = J.skip;
+    C.cdef_idx = J.cdef_idx;
+    C.cdef_stride = J.cdef_stride;
+    C.cdef_count = J.cdef_idx ? J.cdef_count : 0;
+    C.params = J.cdef;
+    C.status = status;
+    return launch_cdef_frame(C, s);
+}
+
 }  // namespace
 
 extern "C" int32_t vaco_av1_ctx_set_tuning(vaco_av1_ctx* ctx, const vaco_av1_tuning* t) {
     if (!ctx || !t) return VACO_AV1_INVALID_DATA;
     if (t->dbcdef_ctas_per_sm < 1 || t->dbcdef_ctas_per_sm > 8 || t->lr_ctas_per_sm < 1 || t->lr_ctas_per_sm > 8 ||
-        !(t->dbcdef_threads == 0 || t->dbcdef_threads == 128 || t->dbcdef_threads == 256))
+        !(t->dbcdef_threads == 0 || t->dbcdef_threads == 128 || t->dbcdef_threads == 256) ||
+        t->stage_fusion < 0 || t->stage_fusion > 1)
         return VACO_AV1_INVALID_DATA;
     ctx->tuning = *t;
     return VACO_AV1_OK;
@@ -130,6 +204,11 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
         e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
         if (e != cudaSuccess) return fail(ctx, e, statuses, msgs, n);
     }
+
+    // Stage fusion (tuning): deblocking and CDEF in the one fused kernel, or
+    // as the per-stage kernels, frame by frame, with the whole deblocked
+    // picture kept for restoration.
+    const bool fused = ctx->tuning.stage_fusion != 0;
 
     // ---- host pass: checks, scratch layout, tile counts
     std::vector<FramePlan> plan(n);
@@ -190,6 +269,8 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
         }
         // scratch: CDEF planes, then (restoration) boundary rows, then superres copies
         for (int k = 0; k < F.np; ++k) F.cdef[k] = arena.take(J.src.width[k], J.src.height[k]);
+        if (!fused)
+            for (int k = 0; k < F.np; ++k) F.deb[k] = arena.take(J.src.width[k], J.src.height[k]);
         F.tiles_db = dbcdef_tiles(info);
         signature += std::to_string(info.coded_width) + "x" + std::to_string(info.coded_height) + "/" +
                      std::to_string(info.upscaled_width) + "/" + std::to_string(info.bit_depth) +
@@ -201,7 +282,7 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     // boundary rows (restoration's pre-CDEF source) of every frame
     for (int i = 0; i < n; ++i) {
         FramePlan& F = plan[i];
-        if (!F.run_db || !F.lr_active) continue;
+        if (!F.run_db || !F.lr_active || !fused) continue;
         for (int k = 0; k < F.np; ++k)
             F.rows[k] = arena.take(jobs[i].src.width[k], pre_rows_count(jobs[i].src.height[k], k ? jobs[i].info.subsampling_y : 0));
     }
@@ -213,7 +294,8 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
             const int sx = k ? info.subsampling_x : 0, sy = k ? info.subsampling_y : 0;
             const int w = (info.upscaled_width + sx) >> sx, h = (info.coded_height + sy) >> sy;
             F.ucdef[k] = arena.take(w, h);
-            if (F.lr_active) F.urows[k] = arena.take(w, F.rows[k].h);
+            if (F.lr_active && fused) F.urows[k] = arena.take(w, F.rows[k].h);
+            if (F.lr_active && !fused) F.udeb[k] = arena.take(w, h);
         }
     }
     unsigned char* base = static_cast<unsigned char*>(ctx->scratch(S_BATCH_ARENA, arena.used));
@@ -274,7 +356,7 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     size_t smem_db = 0;
     int* db_prefix = reinterpret_cast<int*>(htab + off_db_prefix);
     db_prefix[0] = 0;
-    for (size_t q = 0; q < order.size(); ++q) {
+    for (size_t q = 0; q < order.size() && fused; ++q) {
         const int i = order[q];
         const FramePlan& F = plan[i];
         const vaco_av1_frame_job& J = jobs[i];
@@ -339,7 +421,12 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
                 p.copy_only = 1;
             } else {
                 const int u = J.lr_unit_size[k];
-                p.before_rows = dev_cplane(base, F.superres ? F.urows[k] : F.rows[k]);
+                if (fused) {
+                    p.before_rows = dev_cplane(base, F.superres ? F.urows[k] : F.rows[k]);
+                } else {
+                    p.before = dev_cplane(base, F.superres ? F.udeb[k] : F.deb[k]);
+                    p.before_rows = DevPlaneC{nullptr, 0, 0, 0};
+                }
                 p.unit_size = u;
                 p.units = J.lr_units[k];
                 p.unit_cols = std::max((w + u / 2) / u, 1);
@@ -357,7 +444,11 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     const int grid_lr = std::max(1, ctx->sm_count * ctx->tuning.lr_ctas_per_sm);
     auto enqueue = [&]() -> cudaError_t {
         cudaError_t r = cudaMemcpyAsync(dtab, htab, table_bytes, cudaMemcpyHostToDevice, s);
-        if (r == cudaSuccess && !order.empty() && db_prefix[order.size()] > 0)
+        for (int i : order) {  // unfused: deblocking then CDEF, frame by frame
+            if (r != cudaSuccess || fused) break;
+            r = enqueue_unfused(jobs[i], plan[i], base, dstatus + i, s);
+        }
+        if (r == cudaSuccess && fused && !order.empty() && db_prefix[order.size()] > 0)
             r = launch_dbcdef_batch(dtab + off_db, reinterpret_cast<const int*>(dtab + off_db_prefix), (int)order.size(),
                                     reinterpret_cast<int*>(dtab + off_queue), smem_db, grid_db,
                                     ctx->tuning.dbcdef_ctas_per_sm, ctx->tuning.dbcdef_threads, s);
@@ -375,7 +466,15 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
                 sp[k].output_width = (info.upscaled_width + sx) >> sx;
                 sp[k].height = (info.coded_height + sy) >> sy;
             }
-            if (F.lr_active && F.run_lr) {
+            if (F.lr_active && F.run_lr && !fused) {
+                // the whole deblocked picture, in the same launch
+                for (int k = 0; k < F.np; ++k) {
+                    sp[F.np + k] = sp[k];
+                    sp[F.np + k].in = dev_cplane(base, F.deb[k]);
+                    sp[F.np + k].out = dev_plane(base, F.udeb[k]);
+                }
+                nsp = 2 * F.np;
+            } else if (F.lr_active && F.run_lr) {
                 // only the rows the fused kernel wrote (indices 4 .. 4+n), in the same launch
                 for (int k = 0; k < F.np; ++k) {
                     const int n_rows = pre_rows_written(jobs[i].src.height[k], k ? info.subsampling_y : 0);
@@ -402,13 +501,18 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
         return r;
     };
     // kernel launches of this batch: deblock+CDEF, superres, restoration
-    size_t launches = (order.empty() ? 0 : 1) + (lr_order.empty() ? 0 : 1);
-    for (int i : order) launches += plan[i].superres ? 1 : 0;
+    size_t launches = (order.empty() || !fused ? 0 : 1) + (lr_order.empty() ? 0 : 1);
+    for (int i : order) {
+        launches += plan[i].superres ? 1 : 0;
+        if (!fused)  // copy + checks (1 + planes), two passes, CDEF
+            launches += 1 + plan[i].np + (jobs[i].deblock.levels[0] || jobs[i].deblock.levels[1] ? 2 : 0) + 1;
+    }
     ctx->mark(0, s);
     const bool graphs = ctx->tuning.use_graphs && s != nullptr;
     if (graphs) {
         signature += "@" + std::to_string(ctx->scratch_generation) + "/" + std::to_string(grid_db) + "/" +
-                     std::to_string(grid_lr) + "/" + std::to_string(ctx->tuning.largest_first);
+                     std::to_string(grid_lr) + "/" + std::to_string(ctx->tuning.largest_first) + "/" +
+                     std::to_string(ctx->tuning.dbcdef_threads) + "/" + std::to_string(ctx->tuning.stage_fusion);
         auto it = ctx->graphs.find(signature);
         if (it == ctx->graphs.end()) {
             // kernel attributes are set outside the capture

@@ -100,7 +100,7 @@ struct vaco_av1_ctx {
     uint64_t grain_next = 0;
 
     // batched form (batch.cu)
-    vaco_av1_tuning tuning = {3, 4, 1, 1, 256};
+    vaco_av1_tuning tuning = {3, 4, 1, 1, 256, 1};
     unsigned char* batch_table_host = nullptr;   // pinned staging of the per-batch tables
     size_t batch_table_host_bytes = 0;
     unsigned long long* batch_status_host = nullptr;  // pinned copy of the per-frame status words

@@ -242,11 +242,11 @@ class Context:
         return t
 
     def set_tuning(self, dbcdef_ctas_per_sm=None, lr_ctas_per_sm=None, use_graphs=None, largest_first=None,
-                   dbcdef_threads=None):
+                   dbcdef_threads=None, stage_fusion=None):
         t = self.tuning
         for name, v in (("dbcdef_ctas_per_sm", dbcdef_ctas_per_sm), ("lr_ctas_per_sm", lr_ctas_per_sm),
                         ("use_graphs", use_graphs), ("largest_first", largest_first),
-                        ("dbcdef_threads", dbcdef_threads)):
+                        ("dbcdef_threads", dbcdef_threads), ("stage_fusion", stage_fusion)):
             if v is not None:
                 setattr(t, name, int(v))
         st = lib().vaco_av1_ctx_set_tuning(self.handle, C.byref(t))
