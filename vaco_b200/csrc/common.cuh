@@ -42,7 +42,9 @@ __device__ __forceinline__ void report_error(DeviceStatus* st, unsigned stage,
 // previous kernel has completed and its writes are visible, so every read and
 // write after it is ordered exactly as with a plain launch.  Only the launch
 // latency and the CTA start-up overlap the previous kernel's tail.  Without
-// the launch attribute both instructions are no-ops.
+// the launch attribute both instructions are no-ops.  While the stream is
+// being captured into a CUDA graph the launch is a plain one, so captured
+// graphs hold only ordinary dependencies.
 __device__ __forceinline__ void overlap_prologue() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -59,8 +61,10 @@ inline cudaError_t launch_overlapped(void (*kernel)(Params...), dim3 grid, dim3 
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    const bool plain = cudaStreamIsCapturing(stream, &capture) != cudaSuccess || capture != cudaStreamCaptureStatusNone;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = plain ? 0 : 1;
     return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
