@@ -727,6 +727,7 @@ __global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_batch_kernel(const DbCdef
     __shared__ int s_tile, s_frame;
     __shared__ DbCdefArgs s_args;
     const int total = tile_prefix[n];
+    int have = -1;  // frame whose record s_args holds (uniform over the CTA)
     for (;;) {
         __syncthreads();  // previous tile done with shared memory
         if (threadIdx.x == 0) {
@@ -743,13 +744,14 @@ __global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_batch_kernel(const DbCdef
         const int t = s_tile;
         if (t >= total) break;
         const int f = s_frame;
-        {
+        if (f != have) {  // consecutive tiles mostly share a frame: copy its record once
+            have = f;
             const int words = (int)(sizeof(DbCdefArgs) / sizeof(int));
             const int* src = reinterpret_cast<const int*>(frames + f);
             int* dst = reinterpret_cast<int*>(&s_args);
             for (int i = threadIdx.x; i < words; i += NT) dst[i] = src[i];
+            __syncthreads();
         }
-        __syncthreads();
         const int local = t - tile_prefix[f];
         const int tiles_x = (s_args.mi_cols + 15) / 16;
         dbcdef_tile<NT>(s_args, local % tiles_x, local / tiles_x, nullptr);

@@ -571,6 +571,7 @@ __global__ void __launch_bounds__(kLrThreads, 4) restoration_batch_kernel(const 
     __shared__ int s_tile, s_frame;
     __shared__ LrArgs s_args;
     const int total = tile_prefix[n];
+    int have = -1;  // frame whose record s_args holds (uniform over the CTA)
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -587,13 +588,14 @@ __global__ void __launch_bounds__(kLrThreads, 4) restoration_batch_kernel(const 
         const int t = s_tile;
         if (t >= total) break;
         const int f = s_frame;
-        {
+        if (f != have) {  // consecutive tiles mostly share a frame: copy its record once
+            have = f;
             const int words = (int)(sizeof(LrArgs) / sizeof(int));
             const int* src = reinterpret_cast<const int*>(frames + f);
             int* dst = reinterpret_cast<int*>(&s_args);
             for (int i = threadIdx.x; i < words; i += kLrThreads) dst[i] = src[i];
+            __syncthreads();
         }
-        __syncthreads();
         lr_tile(s_args, t - tile_prefix[f]);
     }
 }
