@@ -494,7 +494,7 @@ VACO_AV1_API int32_t vaco_av1_server_submit(vaco_av1_server* server, int32_t str
  * carries host pointers to the reconstruction, side information and
  * restoration units (extents as the stream's, as for
  * vaco_av1_server_upload) together with the frame-level parameters.  The
- * copies into the slot are enqueued on the server's own copy stream and the
+ * copies into the slot are enqueued on the server's own copy streams and the
  * launch that takes the frame waits for them on the device, so one frame's
  * upload overlaps other frames' filtering and the ticket's latency includes
  * the upload.  Host buffers must stay valid until the ticket's wait returns;

@@ -96,7 +96,10 @@ struct vaco_av1_server {
     std::vector<LaunchSlot> launch;
     uint64_t next_ticket = 1;
     int64_t resident = 0, stream_budget = 0, scratch_share = 0;
-    cudaStream_t upload_stream = nullptr;  // host->device copies of submit_host
+    // host->device copies of submit_host, spread over a few copy streams (by
+    // slot) so one frame's copies overlap the set-up of another's
+    static constexpr int kUploadStreams = 4;
+    cudaStream_t upload_streams[kUploadStreams] = {};
     int wait_polls = kDefaultWaitPolls;      // bound of submit / close_stream waits
     vaco_av1_server_stats stats{};
     bool stop = false;
@@ -215,10 +218,11 @@ extern "C" int32_t vaco_av1_server_create(const vaco_av1_server_config* config, 
     s->stream_budget = config->memory_budget_bytes - scratch_total;
     s->stats.scratch_bytes = scratch_total;
     s->launch.resize(config->inflight_batches);
-    if (cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking) != cudaSuccess) {
-        vaco_av1_server_destroy(s);
-        return VACO_AV1_DEVICE_ERROR;
-    }
+    for (cudaStream_t& us : s->upload_streams)
+        if (cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking) != cudaSuccess) {
+            vaco_av1_server_destroy(s);
+            return VACO_AV1_DEVICE_ERROR;
+        }
     for (LaunchSlot& ls : s->launch) {
         if (vaco_av1_ctx_create(config->device, &ls.ctx) != VACO_AV1_OK ||
             cudaEventCreateWithFlags(&ls.done, cudaEventDisableTiming) != cudaSuccess) {
@@ -252,7 +256,8 @@ extern "C" void vaco_av1_server_destroy(vaco_av1_server* s) {
         if (ls.ctx) vaco_av1_ctx_destroy(ls.ctx);
     }
     for (StreamState& st : s->streams) free_stream(st);
-    if (s->upload_stream) cudaStreamDestroy(s->upload_stream);
+    for (cudaStream_t us : s->upload_streams)
+        if (us) cudaStreamDestroy(us);
     delete s;
 }
 
@@ -520,8 +525,9 @@ extern "C" int32_t vaco_av1_server_submit_host(vaco_av1_server* s, int32_t id, i
     // copies are enqueued without the lock.
     lk.unlock();
     cudaSetDevice(s->cfg.device);
-    cudaError_t e = enqueue_upload(d, host, s->upload_stream);
-    if (e == cudaSuccess) e = cudaEventRecord(ev, s->upload_stream);
+    const cudaStream_t us = s->upload_streams[(id + slot) % vaco_av1_server::kUploadStreams];
+    cudaError_t e = enqueue_upload(d, host, us);
+    if (e == cudaSuccess) e = cudaEventRecord(ev, us);
     lk.lock();
     if (e != cudaSuccess) {
         s->streams[id].slots[slot].in_flight = false;
@@ -575,8 +581,8 @@ extern "C" int32_t vaco_av1_server_upload(vaco_av1_server* s, int32_t id, int32_
     if (vaco_av1_server_slot(s, id, slot, &d) != VACO_AV1_OK) return VACO_AV1_INVALID_DATA;
     if (!host_frame_fits(d, host)) return VACO_AV1_INVALID_DATA;
     cudaSetDevice(s->cfg.device);
-    cudaError_t e = enqueue_upload(d, host, s->upload_stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->upload_stream);
+    cudaError_t e = enqueue_upload(d, host, s->upload_streams[0]);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->upload_streams[0]);
     return e == cudaSuccess ? VACO_AV1_OK : VACO_AV1_DEVICE_ERROR;
 }
 
