@@ -23,9 +23,6 @@
 //   [y0-7, y0+th+7) for luma and [y0-3, y0+th+3) for chroma, which is where
 //   the vertical pass must run.  Vertical edges read columns [X-7, X+6].
 // The staged region is [x0-8, x0+tw+8) x [y0-8, y0+th+8).
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include <algorithm>
 #include <atomic>
 #include <cstring>
@@ -112,51 +109,6 @@ struct DbCdefArgs {
     int vec_ok;
     size_t plane_off[3];        // shared-memory offset (samples) of each staged plane
 };
-
-// Tensor maps of a frame's input planes for staging interior tiles with TMA
-// (use == 0: every tile stages with cp.async).  A kernel parameter, so the
-// maps sit in parameter space where the tensor copies read them.
-struct alignas(64) DbCdefTma {
-    CUtensorMap map[3];
-    int use;
-};
-
-// Bound of the wait for a tile's tensor copies: try_wait suspends for a
-// system-dependent time per call, so this is far beyond any copy's latency.
-constexpr int kTmaWaitIters = 1 << 22;
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    return ok != 0;
-}
-
-// One 2-D box of `map` with its first element at (x, y) into shared memory
-// at `dst` (128-byte aligned), completing on `bar`.  x * 2 bytes is a
-// multiple of 16 (x is a multiple of 8 samples) and the whole box lies inside
-// the plane; the source is this GPU's own memory and no multicast is used.
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            smem_u32(dst)),
-        "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
 
 // CDEF output of one plane tile from the staged (deblocked) samples: one warp
 // filters block row br; lane l owns pixel pairs at tile column 2*(l % ppr),
@@ -373,10 +325,9 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
 // CTA calls it; it ends with all threads past their last shared-memory use
 // only after the caller's next __syncthreads().
 template <int NT>
-__device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int tile_y, const DbCdefTma* tma) {
+__device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int tile_y) {
     constexpr int kWarpsNT = NT / 32;
-    extern __shared__ __align__(128) uint16_t smem[];
-    __shared__ uint64_t s_mbar;
+    extern __shared__ __align__(16) uint16_t smem[];
     __shared__ int s_cost[64][8];
     __shared__ PairBlock s_pair[3][64];
     __shared__ uint8_t s_active[64];
@@ -413,37 +364,13 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         s_active[tid] = act;
     }
 
-    // ---- every plane's tile with an 8-sample halo (edge-clamped).  When the
-    // staged region lies inside every plane, one thread stages each plane's
-    // box with a tensor copy (TMA).  Otherwise whole 16-byte chunks inside the
-    // plane go by cp.async, all in flight at once; chunks that straddle the
-    // left/right plane edge are gathered sample by sample, and rows past the
-    // top/bottom edge repeat the edge row.
-    bool tma_tile = tma != nullptr && tma->use;
-    for (int p = 0; p < a.num_planes && tma_tile; ++p) {
-        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
-        const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
-        tma_tile = px0 >= kHalo && py0 >= kHalo && px0 + g.tw + kHalo <= a.src[p].width &&
-                   py0 + g.th + kHalo <= a.src[p].height && (smem_u32(smem + a.plane_off[p]) & 127) == 0;
-    }
-    if (tma_tile) {  // uniform over the CTA
-        if (tid == 0) mbar_init(&s_mbar, 1);
-        __syncthreads();
-        if (tid == 0) {
-            unsigned bytes = 0;
-            for (int p = 0; p < a.num_planes; ++p) {
-                const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
-                bytes += (unsigned)(g.pitch * g.rows * 2);
-            }
-            mbar_expect_tx(&s_mbar, bytes);
-            for (int p = 0; p < a.num_planes; ++p) {
-                const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
-                tma_load_2d(smem + a.plane_off[p], &tma->map[p], (x0 >> g.sx) - kHalo, (y0 >> g.sy) - kHalo,
-                            &s_mbar);
-            }
-        }
-    }
-    for (int p = 0; p < a.num_planes && !tma_tile; ++p) {
+    // ---- every plane's tile with an 8-sample halo (edge-clamped).  Whole
+    // 16-byte chunks inside the plane go by cp.async, all in flight at once;
+    // chunks that straddle the left/right plane edge are gathered sample by
+    // sample.  Rows past the top/bottom edge repeat the edge row.  (Staging
+    // interior tiles with 2-D tensor copies instead measured 1.4 % slower
+    // for the whole chain: the extra path costs more than the copies save.)
+    for (int p = 0; p < a.num_planes; ++p) {
         const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
         const DevPlaneC& P = a.src[p];
         uint16_t* t = smem + a.plane_off[p];
@@ -484,18 +411,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
                 s_side.tx[1][i] = __ldg(a.tx_chroma + (long)(cr0 + wr) * ccols + cc0 + wc);
         }
     }
-    if (tma_tile) {
-        bool done = false;
-        for (int it = 0; it < kTmaWaitIters && !done; ++it) done = mbar_try_wait(&s_mbar, 0);
-        if (!done) {
-            // The copies never completed: fail the frame, then wait once more
-            // (bounded) so no copy is left writing this CTA's shared memory.
-            report_error(a.status, STAGE_DEBLOCK, 0, VACO_AV1_MSG_TIMEOUT);
-            for (int it = 0; it < kTmaWaitIters && !done; ++it) done = mbar_try_wait(&s_mbar, 0);
-        }
-    } else {
-        asm volatile("cp.async.wait_all;\n" ::: "memory");
-    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     const bool any_active = __syncthreads_or(act);
 
     // ---- input checks from shared memory: the tile's own cells (transform
@@ -711,9 +627,9 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
 // SM; at 3 per SM they take two).  128 threads at 5 CTAs per SM is the
 // smaller-CTA shape: shorter barriers, about the same warps per SM.
 template <int NT, int MIN_CTAS>
-__global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_kernel(DbCdefArgs a, const __grid_constant__ DbCdefTma tma) {
+__global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_kernel(DbCdefArgs a) {
     overlap_prologue();
-    dbcdef_tile<NT>(a, blockIdx.x, blockIdx.y, &tma);
+    dbcdef_tile<NT>(a, blockIdx.x, blockIdx.y);
 }
 
 // Persistent form: CTAs take tiles of all frames of a batch from a device
@@ -754,7 +670,7 @@ __global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_batch_kernel(const DbCdef
         }
         const int local = t - tile_prefix[f];
         const int tiles_x = (s_args.mi_cols + 15) / 16;
-        dbcdef_tile<NT>(s_args, local % tiles_x, local / tiles_x, nullptr);
+        dbcdef_tile<NT>(s_args, local % tiles_x, local / tiles_x);
     }
 }
 
@@ -840,57 +756,13 @@ cudaError_t dbcdef_kernel_attributes() {
     return cudaSuccess;
 }
 
-namespace {
-
-// cuTensorMapEncodeTiled from the driver, resolved once through the runtime
-// (no link against the driver library); null when unavailable.
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static std::atomic<void*> fn{nullptr};
-    static std::atomic<int> tried{0};
-    void* f = fn.load(std::memory_order_acquire);
-    if (f || tried.load(std::memory_order_acquire)) return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-    void* p = nullptr;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess && p)
-        fn.store(p, std::memory_order_release);
-    tried.store(1, std::memory_order_release);
-    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn.load(std::memory_order_acquire));
-}
-
-// Tensor maps over the frame's input planes with the staged box of each
-// plane (pitch x rows of the tile plus its halo); use = 0 when the planes
-// cannot be described (alignment) or the encoder is unavailable.
-void build_tma(const DbCdefArgs& a, DbCdefTma* t) {
-    memset(t, 0, sizeof *t);
-    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
-    if (!encode || !a.vec_ok) return;  // vec_ok: 16-byte base and a stride of whole 16-byte units
-    for (int p = 0; p < a.num_planes; ++p) {
-        const int sx = p ? a.ssx : 0, sy = p ? a.ssy : 0;
-        const cuuint64_t dims[2] = {(cuuint64_t)a.src[p].width, (cuuint64_t)a.src[p].height};
-        const cuuint64_t strides[1] = {(cuuint64_t)a.src[p].stride * 2};
-        const cuuint32_t box[2] = {(cuuint32_t)((64 >> sx) + 2 * kHalo), (cuuint32_t)((64 >> sy) + 2 * kHalo)};
-        const cuuint32_t elem[2] = {1, 1};
-        if (a.src[p].width <= 0 || a.src[p].height <= 0 ||
-            encode(&t->map[p], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<uint16_t*>(a.src[p].data), dims, strides,
-                   box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-            return;
-    }
-    t->use = 1;
-}
-
-}  // namespace
-
 cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
     DbCdefArgs a;
     const size_t smem = build_dbcdef_args(L, &a);
-    DbCdefTma tma;
-    build_tma(a, &tma);
     cudaError_t e = dbcdef_kernel_attributes();
     if (e != cudaSuccess) return e;
     dim3 grid(div_up(L.info.mi_cols, 16), div_up(L.info.mi_rows, 16));
-    if (L.threads == 128) return launch_overlapped(dbcdef_kernel<128, 5>, grid, dim3(128), smem, stream, a, tma);
+    if (L.threads == 128) return launch_overlapped(dbcdef_kernel<128, 5>, grid, dim3(128), smem, stream, a);
     // 256 threads: 3 CTAs per SM once the frame has more than 2.5 waves of 4
     // per SM (measured best on 4K and 2880-wide frames; 4 on 1080p and
     // 2560-wide).
@@ -903,8 +775,8 @@ cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
         if (n > 0) sms = n;
     }
     if ((long)grid.x * grid.y * 2 > 5L * 4 * sms)
-        return launch_overlapped(dbcdef_kernel<256, 3>, grid, dim3(256), smem, stream, a, tma);
-    return launch_overlapped(dbcdef_kernel<256, 4>, grid, dim3(256), smem, stream, a, tma);
+        return launch_overlapped(dbcdef_kernel<256, 3>, grid, dim3(256), smem, stream, a);
+    return launch_overlapped(dbcdef_kernel<256, 4>, grid, dim3(256), smem, stream, a);
 }
 
 cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, size_t smem,
