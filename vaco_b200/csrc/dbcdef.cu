@@ -644,17 +644,22 @@ __global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_batch_kernel(const DbCdef
     __shared__ DbCdefArgs s_args;
     const int total = tile_prefix[n];
     int have = -1;  // frame whose record s_args holds (uniform over the CTA)
+    // Thread 0 keeps the next tile index in hand: the atomic for tile k+1 is
+    // issued when tile k starts, so its latency hides behind tile k's work.
+    // A CTA takes tiles in increasing order, so the frame of a tile is found
+    // by stepping forward from the previous tile's frame.
+    int next = 0, frame = 0;
+    if (threadIdx.x == 0) next = atomicAdd(queue, 1);
     for (;;) {
         __syncthreads();  // previous tile done with shared memory
         if (threadIdx.x == 0) {
-            const int t = atomicAdd(queue, 1);
-            int lo = 0, hi = n - 1;  // last frame whose first tile is <= t
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (tile_prefix[mid] <= t) lo = mid; else hi = mid - 1;
+            const int t = next;
+            if (t < total) {
+                while (frame + 1 < n && tile_prefix[frame + 1] <= t) ++frame;
+                next = atomicAdd(queue, 1);
             }
             s_tile = t;
-            s_frame = lo;
+            s_frame = frame;
         }
         __syncthreads();
         const int t = s_tile;
