@@ -402,10 +402,14 @@ VACO_AV1_API int32_t vaco_av1_postfilter_frame_host(vaco_av1_ctx* ctx, const vac
 /* Launch-shape knobs for the batched form (no counterpart in vaco).  The
  * values in tuned/ are picked by vaco_b200.autotune on the target GPU. */
 typedef struct vaco_av1_tuning {
-    int32_t dbcdef_ctas_per_sm;  /* persistent CTAs per SM, deblock+CDEF kernel (1..4) */
-    int32_t lr_ctas_per_sm;      /* persistent CTAs per SM, restoration kernel (1..4) */
+    int32_t dbcdef_ctas_per_sm;  /* resident CTAs per SM the batched deblock+CDEF kernel
+                                    is compiled for, i.e. its register budget (1..8):
+                                    up to 3 -> 80 registers a thread, 4 and more -> 64
+                                    (256-thread tiles; 128-thread tiles have one body) */
+    int32_t lr_ctas_per_sm;      /* the same for the batched restoration kernel (1..8):
+                                    up to 3 -> 80 registers, 4 and more -> 64 */
     int32_t use_graphs;          /* capture each batch composition once as a CUDA graph */
-    int32_t largest_first;       /* queue the largest frames' tiles first */
+    int32_t largest_first;       /* lay the largest frames' tiles first in the launch */
     int32_t dbcdef_threads;      /* threads per 64x64 tile of the deblock+CDEF kernel, in the
                                     batched form and vaco_av1_postfilter_frame_dev: 256 or
                                     128 (0 = 256) */
@@ -420,8 +424,8 @@ VACO_AV1_API int32_t vaco_av1_ctx_get_tuning(const vaco_av1_ctx* ctx, vaco_av1_t
 /* The chain over `n` frames of any sizes and bit depths in one launch set
  * (no counterpart in vaco, which filters one frame per decode_frame call,
  * src/decode.rs:553-559).  Pointers in `jobs` are device pointers.
- * Deblock+CDEF and restoration each run as one persistent kernel whose CTAs
- * take superblock tiles of all frames from a device-side queue; every frame
+ * Deblock+CDEF and restoration each run as one kernel launch with one CTA
+ * per tile of all frames, the frames' tiles laid end to end; every frame
  * keeps its own status word.  statuses[i] / msgs[i] (both optional) receive
  * frame i's result; the return value is VACO_AV1_OK when every frame
  * succeeded, else the status of the first failing frame.  Synchronizes

@@ -1,7 +1,7 @@
 """The batched form: many frames of different sizes and bit depths in one
-launch set (persistent per-stage kernels over a device tile queue, optionally
-replayed from a CUDA graph) give, frame by frame, exactly the single-frame
-results and the oracle's."""
+launch set (one per-stage kernel launch over the tiles of all frames,
+optionally replayed from a CUDA graph) give, frame by frame, exactly the
+single-frame results and the oracle's."""
 import numpy as np
 import pytest
 import torch
@@ -90,12 +90,14 @@ def test_config3_full_mix_matches_oracle(ctx, oracle_threads):
             assert np.array_equal(g, w), f"frame {i} ({f.coded_width}x{f.coded_height}) plane {k} differs"
 
 
-@pytest.mark.parametrize("shape", [(256, 3, 1), (128, 5, 1), (256, 4, 0)], ids=["fused256", "fused128", "unfused"])
+@pytest.mark.parametrize("shape", [(256, 3, 1, 4), (256, 4, 1, 3), (128, 5, 1, 4), (256, 4, 0, 4)],
+                         ids=["fused256x3", "fused256x4_lr3", "fused128", "unfused"])
 def test_batch_launch_shapes_and_stage_fusion_match_oracle(ctx, shape, oracle_threads):
-    """Every launch shape and stage-fusion choice the autotuner may pick gives
+    """Every kernel body and stage-fusion choice the autotuner may pick gives
     the oracle's planes (superres frames and restoration included)."""
-    threads, ctas, fusion = shape
-    ctx.set_tuning(dbcdef_threads=threads, dbcdef_ctas_per_sm=ctas, stage_fusion=fusion, use_graphs=1)
+    threads, ctas, fusion, lr_ctas = shape
+    ctx.set_tuning(dbcdef_threads=threads, dbcdef_ctas_per_sm=ctas, stage_fusion=fusion, use_graphs=1,
+                   lr_ctas_per_sm=lr_ctas)
     try:
         frames = mixed_frames(900)
         devs = [DeviceFrame(f) for f in frames]
@@ -107,7 +109,7 @@ def test_batch_launch_shapes_and_stage_fusion_match_oracle(ctx, shape, oracle_th
             for g, w in zip(d.outputs_numpy(), want):
                 np.testing.assert_array_equal(g, w)
     finally:
-        ctx.set_tuning(dbcdef_threads=256, dbcdef_ctas_per_sm=3, stage_fusion=1)
+        ctx.set_tuning(dbcdef_threads=256, dbcdef_ctas_per_sm=3, stage_fusion=1, lr_ctas_per_sm=4)
 
 
 def test_per_frame_128_thread_tiles_match_oracle(ctx, oracle_threads):

@@ -14,6 +14,9 @@ pytestmark = pytest.mark.gpu
 SMALL = [  # (width, height, bit_depth, upscaled_width)
     (64, 64, 8, None), (200, 136, 10, None), (96, 80, 12, None), (328, 200, 10, 400),
     (120, 72, 8, 136), (520, 264, 10, None),
+    # coded sizes that are not multiples of 8 (the planes are mi-aligned,
+    # the chain's outputs are cropped to the coded / upscaled size)
+    (60, 44, 10, None), (204, 130, 8, None), (118, 70, 12, None), (100, 58, 10, 124),
 ]
 
 

@@ -2,10 +2,11 @@
 
 Sweeps, with CUDA-event timing on the target GPU:
   batch  (64 mixed frames, config 3): threads per 64x64 tile of the fused
-         deblock+CDEF kernel (256 or 128) with its persistent CTAs per SM,
-         the restoration kernel's persistent CTAs per SM, CUDA-graph replay,
-         the tile-queue order, and the stage fusion (deblocking and CDEF in
-         one kernel, or as separate kernels);
+         deblock+CDEF kernel (256 or 128) with the resident CTAs per SM its
+         body is compiled for (its register budget), the same for the
+         restoration kernel, CUDA-graph replay, the frames' tile order, and
+         the stage fusion (deblocking and CDEF in one kernel, or as separate
+         kernels);
   frame  (4K 10-bit frames back to back): threads per tile of the fused
          kernel on the per-frame path.
 and writes the fastest settings to tuned/<gpu>.json, which load_tuning()
@@ -48,9 +49,10 @@ def load_tuning() -> dict:
     return dict(DEFAULT)
 
 
-# (threads per tile, persistent CTAs per SM) of the fused kernel: 256-thread
-# tiles at 2-4 per SM, 128-thread tiles at 4-6 (about the same warps per SM)
-DBCDEF_SHAPES = ((256, 2), (256, 3), (256, 4), (128, 4), (128, 5), (128, 6))
+# (threads per tile, resident CTAs per SM its body is compiled for) of the
+# fused kernel: the three bodies there are (256 threads at 80 or 64 registers,
+# 128 threads at 5 per SM)
+DBCDEF_SHAPES = ((256, 3), (256, 4), (128, 5))
 
 
 def _time(fn, reps, stream):

@@ -4,13 +4,13 @@
 // src/decode.rs:553-559).  Here a batch of frames of any sizes and bit depths
 // shares one launch set:
 //   1. one upload of the per-batch tables (frame argument records, tile
-//      prefix sums, initial status words, queue counters)
-//   2. one persistent deblock+CDEF kernel draining a device tile queue that
-//      spans all frames (dbcdef.cu)
+//      prefix sums, initial status words)
+//   2. one deblock+CDEF kernel with one CTA per tile of all frames
+//      (dbcdef.cu)
 //   3. superres launches for the frames that upscale
-//   4. one persistent restoration kernel over all frames' tiles
-//      (restoration.cu), which also validates every restoration unit and
-//      copies planes whose frame-level restoration is off
+//   4. one restoration kernel over all frames' tiles (restoration.cu), which
+//      also validates every restoration unit and copies planes whose
+//      frame-level restoration is off
 //   5. one download of the per-frame status words
 // With tuning.use_graphs, steps 1-5 are captured once per batch composition as
 // a CUDA graph and replayed afterwards; the tables carry every per-batch
@@ -301,7 +301,7 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     unsigned char* base = static_cast<unsigned char*>(ctx->scratch(S_BATCH_ARENA, arena.used));
     if (!base) return fail(ctx, cudaErrorMemoryAllocation, statuses, msgs, n);
 
-    // ---- queue order: frames that run, largest first when tuned so
+    // ---- tile order: frames that run, largest first when tuned so
     std::vector<int> order;
     for (int i = 0; i < n; ++i)
         if (plan[i].run_db) order.push_back(i);
@@ -316,8 +316,6 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     size_t off = 0;
     const size_t off_status = off;
     off = align_up(off + sizeof(DeviceStatus) * n, 256);
-    const size_t off_queue = off;
-    off = align_up(off + 2 * sizeof(int), 256);
     const size_t off_db = off;
     off = align_up(off + db_rec * order.size(), 256);
     const size_t off_db_prefix = off;
@@ -350,7 +348,6 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     unsigned char* htab = ctx->batch_table_host;
     DeviceStatus* dstatus = reinterpret_cast<DeviceStatus*>(dtab + off_status);
     memset(htab + off_status, 0xFF, sizeof(DeviceStatus) * n);
-    memset(htab + off_queue, 0, 2 * sizeof(int));
 
     // deblock + CDEF records
     size_t smem_db = 0;
@@ -440,8 +437,6 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     }
 
     // ---- the launch sequence (captured once per composition when tuned so)
-    const int grid_db = std::max(1, ctx->sm_count * ctx->tuning.dbcdef_ctas_per_sm);
-    const int grid_lr = std::max(1, ctx->sm_count * ctx->tuning.lr_ctas_per_sm);
     auto enqueue = [&]() -> cudaError_t {
         cudaError_t r = cudaMemcpyAsync(dtab, htab, table_bytes, cudaMemcpyHostToDevice, s);
         for (int i : order) {  // unfused: deblocking then CDEF, frame by frame
@@ -450,8 +445,8 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
         }
         if (r == cudaSuccess && fused && !order.empty() && db_prefix[order.size()] > 0)
             r = launch_dbcdef_batch(dtab + off_db, reinterpret_cast<const int*>(dtab + off_db_prefix), (int)order.size(),
-                                    reinterpret_cast<int*>(dtab + off_queue), smem_db, grid_db,
-                                    ctx->tuning.dbcdef_ctas_per_sm, ctx->tuning.dbcdef_threads, s);
+                                    db_prefix[order.size()], smem_db, ctx->tuning.dbcdef_ctas_per_sm,
+                                    ctx->tuning.dbcdef_threads, s);
         for (int i : order) {
             const FramePlan& F = plan[i];
             if (r != cudaSuccess || !F.superres) continue;
@@ -494,7 +489,8 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
         }
         if (r == cudaSuccess && !lr_order.empty() && lr_prefix[lr_order.size()] > 0)
             r = launch_restoration_batch(dtab + off_lr, reinterpret_cast<const int*>(dtab + off_lr_prefix),
-                                         (int)lr_order.size(), reinterpret_cast<int*>(dtab + off_queue) + 1, grid_lr, s);
+                                         (int)lr_order.size(), lr_prefix[lr_order.size()], ctx->tuning.lr_ctas_per_sm,
+                                         s);
         if (r == cudaSuccess)
             r = cudaMemcpyAsync(ctx->batch_status_host, dstatus, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost,
                                 s);
@@ -510,8 +506,9 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     ctx->mark(0, s);
     const bool graphs = ctx->tuning.use_graphs && s != nullptr;
     if (graphs) {
-        signature += "@" + std::to_string(ctx->scratch_generation) + "/" + std::to_string(grid_db) + "/" +
-                     std::to_string(grid_lr) + "/" + std::to_string(ctx->tuning.largest_first) + "/" +
+        signature += "@" + std::to_string(ctx->scratch_generation) + "/" +
+                     std::to_string(ctx->tuning.dbcdef_ctas_per_sm) + "/" + std::to_string(ctx->tuning.lr_ctas_per_sm) +
+                     "/" + std::to_string(ctx->tuning.largest_first) + "/" +
                      std::to_string(ctx->tuning.dbcdef_threads) + "/" + std::to_string(ctx->tuning.stage_fusion);
         auto it = ctx->graphs.find(signature);
         if (it == ctx->graphs.end()) {

@@ -127,6 +127,21 @@ __device__ __forceinline__ unsigned fast_div(unsigned n, unsigned d, unsigned re
     return q;
 }
 
+// The frame of tile t in a batch whose frames' tiles are laid end to end:
+// the last f in [0, n) with prefix[f] <= t (prefix holds n + 1 running tile
+// counts, prefix[0] = 0; a frame without tiles is never picked, since the
+// next frame starts at the same count).  Every thread of a CTA searches the
+// same entries, so the loads are broadcasts.
+__device__ __forceinline__ int frame_of_tile(const int* __restrict__ prefix, int n, int t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 // Chroma layouts AV1 can signal (color_config, spec 5.5.2): 4:2:0, 4:2:2 and
 // 4:4:4.  subsampling_y is only coded when subsampling_x is 1, so 4:4:0 does
 // not exist; the fused deblock+CDEF tile layout relies on that.

@@ -296,5 +296,334 @@ __device__ __forceinline__ void line_size16(uint16_t* q, long step_rt, int nq, i
     for (int i = -6; i < 6; ++i) store_at<STEP>(q, step_rt, nq, np, i, out[i + 6]);
 }
 
+// ---------------------------------------------------------------- two lines per register
+//
+// The size-class filters above for two adjacent lines of one edge segment at
+// once: sample k of both lines sits in one 32-bit word, the first line in the
+// low 16 bits.  Both lines share the segment's filter size and strengths;
+// each keeps its own masks (filterMask, hev, flat, flat2 of 7.14.6.2), which
+// select per 16-bit half between the original samples and the narrow, 8-tap
+// or 14-tap results, so the lines never diverge.  Every per-half quantity
+// stays in [0, 65535], so plain 32-bit adds and subtracts never carry or
+// borrow across halves:
+//   - samples are at most 4095 (12-bit); |a - b| = max(a, b) - min(a, b);
+//   - the wide filters' weighted sums are at most 16 x 4095 + 8;
+//   - the narrow filter's signed intermediates (7.14.6.3) are held biased by
+//     kNarrowBias = 2^14, whose magnitude exceeds every negative value they
+//     take (|ps1 - qs1| + 3 |qs0 - ps0| <= 4 x 4095), and whose multiples of
+//     8 and 16 keep the arithmetic shifts exact: (v + 2^14) >> 3 =
+//     (v >> 3) + 2^11 for any v > -2^14.
+// The callers use these only where the segment reaches R samples into the
+// plane on both sides (no clamped reads, no dropped writes); nearer the plane
+// edge they run the per-line filters above.
+
+__device__ __forceinline__ uint32_t pmin2(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("min.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t pmax2(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ constexpr uint32_t pk2(int v) { return (uint32_t)v * 0x10001u; }
+__device__ __forceinline__ uint32_t absd2(uint32_t a, uint32_t b) { return pmax2(a, b) - pmin2(a, b); }
+// Per half: non-zero iff a > t.
+__device__ __forceinline__ uint32_t over2(uint32_t a, uint32_t t) { return pmax2(a, t) - t; }
+// Per half: 0xFFFF where x's half is non-zero, else 0.
+__device__ __forceinline__ uint32_t mask2(uint32_t x) { return pmin2(x, 0x00010001u) * 0xFFFFu; }
+// Per half: m ? a : b.
+__device__ __forceinline__ uint32_t sel2(uint32_t m, uint32_t a, uint32_t b) { return (a & m) | (b & ~m); }
+
+constexpr int kNarrowBias = 1 << 14;
+
+// Packed limit / blimit / thresh / flatness bound of a segment (7.14.4),
+// scaled to the bit depth.
+struct PairStrength {
+    uint32_t limit, blimit, thresh, one;
+    int sh;
+};
+
+__device__ __forceinline__ PairStrength pair_strength(const Strength& s, int bd) {
+    const int sh = bd - 8;
+    return PairStrength{pk2(s.limit << sh), pk2(s.blimit << sh), pk2(s.thresh << sh), pk2(1 << sh), sh};
+}
+
+// 2 |p0 - q0| + |p1 - q1| / 2, the blimit side of filterMask.
+__device__ __forceinline__ uint32_t blimit_term2(const uint32_t* P, const uint32_t* Q) {
+    return absd2(P[0], Q[0]) * 2u + ((absd2(P[1], Q[1]) >> 1) & 0x7FFF7FFFu);
+}
+
+// 7.14.6.3 narrow filter of both halves (hevm: 0xFFFF where hev), in place.
+__device__ __forceinline__ void narrow2(uint32_t& p1, uint32_t& p0, uint32_t& q0, uint32_t& q1, uint32_t hevm,
+                                        int sh) {
+    const int half = 0x80 << sh;
+    const uint32_t lo = pk2(kNarrowBias - half), hi = pk2(kNarrowBias + half - 1);
+    // f = hev ? clamp(ps1 - qs1) : 0, then clamp(f + 3 (qs0 - ps0)); biased
+    uint32_t f = sel2(hevm, pmin2(pmax2(p1 + pk2(kNarrowBias) - q1, lo), hi), pk2(kNarrowBias));
+    f = pmin2(pmax2(f + 3u * q0 - 3u * p0, lo), hi);
+    // f1 = clamp(f + 4) >> 3, f2 = clamp(f + 3) >> 3, f3 = (f1 + 1) >> 1, each
+    // plus the bias shifted alike (2^11 for f1 and f2, 2^10 for f3)
+    const uint32_t f1 = (pmin2(f + pk2(4), hi) >> 3) & 0x1FFF1FFFu;
+    const uint32_t f2 = (pmin2(f + pk2(3), hi) >> 3) & 0x1FFF1FFFu;
+    const uint32_t f3 = ((f1 + pk2(1)) >> 1) & 0x7FFF7FFFu;
+    // clamp(qs0 - f1) + half and so on: the biased value minus (bias - half)
+    const uint32_t nq0 = pmin2(pmax2(q0 + pk2(kNarrowBias + kNarrowBias / 8 - half) - f1, lo), hi) - lo;
+    const uint32_t np0 = pmin2(pmax2(p0 + f2 + pk2(kNarrowBias - half - kNarrowBias / 8), lo), hi) - lo;
+    const uint32_t nq1 = pmin2(pmax2(q1 + pk2(kNarrowBias + kNarrowBias / 16 - half) - f3, lo), hi) - lo;
+    const uint32_t np1 = pmin2(pmax2(p1 + f3 + pk2(kNarrowBias - half - kNarrowBias / 16), lo), hi) - lo;
+    q0 = nq0;
+    p0 = np0;
+    q1 = sel2(hevm, q1, nq1);
+    p1 = sel2(hevm, p1, np1);
+}
+
+// Samples -R .. R-1 of the lane's two lines, q at sample 0 of the first line
+// (4-byte aligned).  PASS 1 (horizontal edge): the lines are adjacent
+// columns, so sample k of both is one word k rows away.  PASS 0 (vertical
+// edge): the lines are adjacent rows; words of two samples along each row
+// are interleaved into (row 0, row 1) pairs.  P[k] is sample -(k+1).
+template <int PASS, int R>
+__device__ __forceinline__ void load_pair(const uint16_t* q, int pitch, uint32_t* P, uint32_t* Q) {
+    if (PASS == 1) {
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(q);
+        const int wp = pitch >> 1;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            Q[k] = w[k * wp];
+            P[k] = w[-(k + 1) * wp];
+        }
+    } else {
+        const uint32_t* r0 = reinterpret_cast<const uint32_t*>(q);
+        const uint32_t* r1 = reinterpret_cast<const uint32_t*>(q + pitch);
+#pragma unroll
+        for (int j = 0; j < (R + 1) / 2; ++j) {
+            uint32_t a = r0[j], b = r1[j];  // samples 2j, 2j+1
+            Q[2 * j] = __byte_perm(a, b, 0x5410);
+            if (2 * j + 1 < R) Q[2 * j + 1] = __byte_perm(a, b, 0x7632);
+            a = r0[-(j + 1)];  // samples -2j-2, -2j-1
+            b = r1[-(j + 1)];
+            P[2 * j] = __byte_perm(a, b, 0x7632);
+            if (2 * j + 1 < R) P[2 * j + 1] = __byte_perm(a, b, 0x5410);
+        }
+    }
+}
+
+// Stores samples -NP .. NQ-1 of both lines (the layout of load_pair).  For
+// PASS 0, NP and NQ are even: whole words along each row.
+template <int PASS, int NP, int NQ>
+__device__ __forceinline__ void store_pair(uint16_t* q, int pitch, const uint32_t* P, const uint32_t* Q) {
+    if (PASS == 1) {
+        uint32_t* w = reinterpret_cast<uint32_t*>(q);
+        const int wp = pitch >> 1;
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) w[k * wp] = Q[k];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) w[-(k + 1) * wp] = P[k];
+    } else {
+        uint32_t* r0 = reinterpret_cast<uint32_t*>(q);
+        uint32_t* r1 = reinterpret_cast<uint32_t*>(q + pitch);
+#pragma unroll
+        for (int j = 0; j < NQ / 2; ++j) {
+            r0[j] = __byte_perm(Q[2 * j], Q[2 * j + 1], 0x5410);
+            r1[j] = __byte_perm(Q[2 * j], Q[2 * j + 1], 0x7632);
+        }
+#pragma unroll
+        for (int j = 0; j < NP / 2; ++j) {
+            r0[-(j + 1)] = __byte_perm(P[2 * j + 1], P[2 * j], 0x5410);
+            r1[-(j + 1)] = __byte_perm(P[2 * j + 1], P[2 * j], 0x7632);
+        }
+    }
+}
+
+// The 8-tap outputs (samples -3 .. 2) of apply8 into w[0..5].
+__device__ __forceinline__ void wide8_2(const uint32_t* P, const uint32_t* Q, uint32_t* w) {
+    const uint32_t p3 = P[3], p2 = P[2], p1 = P[1], p0 = P[0], q0 = Q[0], q1 = Q[1], q2 = Q[2], q3 = Q[3];
+    const uint32_t r = pk2(4), m = 0x1FFF1FFFu;
+    w[0] = ((3u * p3 + 2u * p2 + p1 + p0 + q0 + r) >> 3) & m;
+    w[1] = ((2u * p3 + p2 + 2u * p1 + p0 + q0 + q1 + r) >> 3) & m;
+    w[2] = ((p3 + p2 + p1 + 2u * p0 + q0 + q1 + q2 + r) >> 3) & m;
+    w[3] = ((p2 + p1 + p0 + 2u * q0 + q1 + q2 + q3 + r) >> 3) & m;
+    w[4] = ((p1 + p0 + q0 + 2u * q1 + q2 + 2u * q3 + r) >> 3) & m;
+    w[5] = ((p0 + q0 + q1 + 2u * q2 + 3u * q3 + r) >> 3) & m;
+}
+
+// Filter size 4: mask over p1..q1, narrow filter.
+template <int PASS>
+__device__ __forceinline__ void pair_size4(uint16_t* q, int pitch, const PairStrength& s) {
+    uint32_t P[2], Q[2];
+    load_pair<PASS, 2>(q, pitch, P, Q);
+    const uint32_t dpq = pmax2(absd2(P[1], P[0]), absd2(Q[1], Q[0]));
+    const uint32_t keep = mask2(over2(dpq, s.limit) | over2(blimit_term2(P, Q), s.blimit));
+    if (keep == 0xFFFFFFFFu) return;
+    uint32_t p1 = P[1], p0 = P[0], q0 = Q[0], q1 = Q[1];
+    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), s.sh);
+    P[1] = sel2(keep, P[1], p1);
+    P[0] = sel2(keep, P[0], p0);
+    Q[0] = sel2(keep, Q[0], q0);
+    Q[1] = sel2(keep, Q[1], q1);
+    store_pair<PASS, 2, 2>(q, pitch, P, Q);
+}
+
+// Filter size 8 on a chroma plane (filter length 6).
+template <int PASS>
+__device__ __forceinline__ void pair_size6(uint16_t* q, int pitch, const PairStrength& s) {
+    uint32_t P[3], Q[3];
+    load_pair<PASS, 3>(q, pitch, P, Q);
+    const uint32_t dpq = pmax2(absd2(P[1], P[0]), absd2(Q[1], Q[0]));
+    const uint32_t m = pmax2(dpq, pmax2(absd2(P[2], P[1]), absd2(Q[2], Q[1])));
+    const uint32_t keep = mask2(over2(m, s.limit) | over2(blimit_term2(P, Q), s.blimit));
+    if (keep == 0xFFFFFFFFu) return;
+    const uint32_t steep = mask2(over2(pmax2(dpq, pmax2(absd2(P[2], P[0]), absd2(Q[2], Q[0]))), s.one));
+    uint32_t p1 = P[1], p0 = P[0], q0 = Q[0], q1 = Q[1];
+    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), s.sh);
+    if ((~steep & ~keep) != 0) {  // a flat line: the 6-tap filter
+        const uint32_t p2 = P[2], q2 = Q[2], r = pk2(4), mk = 0x1FFF1FFFu;
+        p1 = sel2(steep, p1, ((3u * p2 + 2u * P[1] + 2u * P[0] + Q[0] + r) >> 3) & mk);
+        const uint32_t w0 = ((p2 + 2u * P[1] + 2u * P[0] + 2u * Q[0] + Q[1] + r) >> 3) & mk;
+        const uint32_t w1 = ((P[1] + 2u * P[0] + 2u * Q[0] + 2u * Q[1] + q2 + r) >> 3) & mk;
+        q1 = sel2(steep, q1, ((P[0] + 2u * Q[0] + 2u * Q[1] + 3u * q2 + r) >> 3) & mk);
+        p0 = sel2(steep, p0, w0);
+        q0 = sel2(steep, q0, w1);
+    }
+    P[1] = sel2(keep, P[1], p1);
+    P[0] = sel2(keep, P[0], p0);
+    Q[0] = sel2(keep, Q[0], q0);
+    Q[1] = sel2(keep, Q[1], q1);
+    store_pair<PASS, 2, 2>(q, pitch, P, Q);
+}
+
+// filterMask and the flat mask over p3..q3 (filter sizes 8 and 16 on luma).
+__device__ __forceinline__ void masks8_2(const uint32_t* P, const uint32_t* Q, const PairStrength& s, uint32_t& dpq,
+                                         uint32_t& keep, uint32_t& steep) {
+    dpq = pmax2(absd2(P[1], P[0]), absd2(Q[1], Q[0]));
+    const uint32_t m = pmax2(pmax2(dpq, pmax2(absd2(P[2], P[1]), absd2(Q[2], Q[1]))),
+                             pmax2(absd2(P[3], P[2]), absd2(Q[3], Q[2])));
+    keep = mask2(over2(m, s.limit) | over2(blimit_term2(P, Q), s.blimit));
+    const uint32_t fl = pmax2(pmax2(dpq, pmax2(absd2(P[2], P[0]), absd2(Q[2], Q[0]))),
+                              pmax2(absd2(P[3], P[0]), absd2(Q[3], Q[0])));
+    steep = mask2(over2(fl, s.one));
+}
+
+// Filter size 8 on luma (filter length 8).
+template <int PASS>
+__device__ __forceinline__ void pair_size8(uint16_t* q, int pitch, const PairStrength& s) {
+    uint32_t P[4], Q[4];
+    load_pair<PASS, 4>(q, pitch, P, Q);
+    uint32_t dpq, keep, steep;
+    masks8_2(P, Q, s, dpq, keep, steep);
+    if (keep == 0xFFFFFFFFu) return;
+    uint32_t p1 = P[1], p0 = P[0], q0 = Q[0], q1 = Q[1];
+    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), s.sh);
+    const uint32_t n[4] = {p1, p0, q0, q1};
+    if ((~steep & ~keep) == 0) {  // narrow lines only: samples -2 .. 1
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            P[k] = sel2(keep, P[k], n[1 - k]);
+            Q[k] = sel2(keep, Q[k], n[2 + k]);
+        }
+        store_pair<PASS, 2, 2>(q, pitch, P, Q);
+        return;
+    }
+    uint32_t w[6];
+    wide8_2(P, Q, w);
+    const uint32_t flat = ~steep & ~keep, narrow = steep & ~keep;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {  // samples -(k+1) and k
+        uint32_t pv = sel2(flat, w[2 - k], P[k]), qv = sel2(flat, w[3 + k], Q[k]);
+        if (k < 2) {
+            pv = sel2(narrow, n[1 - k], pv);
+            qv = sel2(narrow, n[2 + k], qv);
+        }
+        P[k] = pv;
+        Q[k] = qv;
+    }
+    store_pair<PASS, PASS == 0 ? 4 : 3, PASS == 0 ? 4 : 3>(q, pitch, P, Q);
+}
+
+// Filter size 16 on luma: narrow, 8-tap or 14-tap by the flat masks.
+template <int PASS>
+__device__ __forceinline__ void pair_size16(uint16_t* q, int pitch, const PairStrength& s) {
+    uint32_t P[7], Q[7];
+    load_pair<PASS, 7>(q, pitch, P, Q);
+    uint32_t dpq, keep, steep;
+    masks8_2(P, Q, s, dpq, keep, steep);
+    if (keep == 0xFFFFFFFFu) return;
+    uint32_t p1 = P[1], p0 = P[0], q0 = Q[0], q1 = Q[1];
+    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), s.sh);
+    const uint32_t n[4] = {p1, p0, q0, q1};
+    const uint32_t flat = ~steep & ~keep, narrow = steep & ~keep;
+    if (flat == 0) {  // narrow lines only: samples -2 .. 1
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            P[k] = sel2(keep, P[k], n[1 - k]);
+            Q[k] = sel2(keep, Q[k], n[2 + k]);
+        }
+        store_pair<PASS, 2, 2>(q, pitch, P, Q);
+        return;
+    }
+    const uint32_t fl2 = pmax2(pmax2(pmax2(absd2(P[6], P[0]), absd2(Q[6], Q[0])),
+                                     pmax2(absd2(P[5], P[0]), absd2(Q[5], Q[0]))),
+                               pmax2(absd2(P[4], P[0]), absd2(Q[4], Q[0])));
+    const uint32_t flat2 = flat & ~mask2(over2(fl2, s.one)), flat1 = flat & ~flat2;
+    uint32_t w[6];
+    wide8_2(P, Q, w);
+    uint32_t o[12];  // outputs of samples -6 .. 5
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        o[5 - k] = P[k];
+        o[6 + k] = Q[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) o[3 + k] = sel2(flat1, w[k], o[3 + k]);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[4 + k] = sel2(narrow, n[k], o[4 + k]);
+    if (flat2 != 0) {
+        // 14-tap (log2Size 4): out[i] = (T_i + F[i-1] + F[i] + F[i+1] + 8) >> 4
+        // with T_i the edge-clamped 13-sample window sum, as line_size16
+        uint32_t F[14];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            F[6 - k] = P[k];
+            F[7 + k] = Q[k];
+        }
+        uint32_t T = 6u * F[0];
+#pragma unroll
+        for (int k = 1; k <= 7; ++k) T += F[k];
+#pragma unroll
+        for (int i = -6; i < 6; ++i) {
+            const int c = i + 7;
+            o[i + 6] = sel2(flat2, ((T + F[c - 1] + F[c] + F[c + 1] + pk2(8)) >> 4) & 0x0FFF0FFFu, o[i + 6]);
+            if (i < 5) T = T + F[min(c + 7, 13)] - F[max(c - 6, 0)];
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            P[k] = o[5 - k];
+            Q[k] = o[6 + k];
+        }
+        store_pair<PASS, 6, 6>(q, pitch, P, Q);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        P[k] = o[5 - k];
+        Q[k] = o[6 + k];
+    }
+    store_pair<PASS, PASS == 0 ? 4 : 3, PASS == 0 ? 4 : 3>(q, pitch, P, Q);
+}
+
+template <int PASS>
+__device__ __forceinline__ void filter_pair_class(int cls, uint16_t* q, int pitch, const PairStrength& s) {
+    if (cls == 0) pair_size4<PASS>(q, pitch, s);
+    else if (cls == 1) pair_size6<PASS>(q, pitch, s);
+    else if (cls == 2) pair_size8<PASS>(q, pitch, s);
+    else pair_size16<PASS>(q, pitch, s);
+}
+
+// Samples per side a size class reads (and the per-line filters' clamping
+// threshold): 4-tap 2, chroma 6-tap 3, luma 8-tap 4, luma 14-tap 7.
+__device__ __forceinline__ int class_reach(int cls) { return cls == 0 ? 2 : cls == 1 ? 3 : cls == 2 ? 4 : 7; }
+
 }  // namespace dbk
 }  // namespace vaco

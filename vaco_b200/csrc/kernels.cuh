@@ -88,7 +88,7 @@ cudaError_t launch_restoration(const LrPlane* planes, int count, int bit_depth, 
 // bytes built by build_lr_args (which returns the frame's tile count).
 size_t lr_args_size();
 int build_lr_args(const LrPlane* planes, int count, int bit_depth, void* out);
-cudaError_t launch_restoration_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, int grid,
+cudaError_t launch_restoration_batch(const void* dev_args, const int* dev_prefix, int n, int tiles, int ctas_per_sm,
                                      cudaStream_t stream);
 // Shared-memory opt-ins of every kernel on the current device (idempotent);
 // call before stream capture.
@@ -151,14 +151,14 @@ struct DbCdefLaunch {
 cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream);
 // Batched form: `dev_args` holds n per-frame argument records (dbcdef_args_size()
 // bytes each, built by build_dbcdef_args), `dev_prefix` n+1 running tile
-// counts, `dev_queue` a zeroed counter.  `grid` persistent CTAs drain the queue;
-// `ctas_per_sm` (grid / SMs) and `threads` (per tile, 256 or 128) pick the
-// kernel body compiled for that shape.
+// counts; one CTA per tile of all n frames (`tiles` = dev_prefix[n]).
+// `ctas_per_sm` (resident CTAs per SM the body is compiled for, i.e. its
+// register budget) and `threads` (per tile, 256 or 128) pick the kernel body.
 size_t dbcdef_args_size();
 size_t build_dbcdef_args(const DbCdefLaunch& L, void* out);  // returns dynamic smem bytes
 inline int dbcdef_tiles(const vaco_av1_frame_info& i) { return ((i.mi_cols + 15) / 16) * ((i.mi_rows + 15) / 16); }
-cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, size_t smem,
-                                int grid, int ctas_per_sm, int threads, cudaStream_t stream);
+cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int n, int tiles, size_t smem,
+                                int ctas_per_sm, int threads, cudaStream_t stream);
 // Rows in the compact boundary buffer of a plane of `height` rows.
 inline int pre_rows_count(int height, int sub_y) {
     const int sh = 64 >> sub_y, off = 8 >> sub_y;

@@ -564,45 +564,15 @@ __global__ void __launch_bounds__(kLrThreads, 4) restoration_kernel(LrArgs a) {
     lr_tile(a, blockIdx.x);
 }
 
-// Persistent form over the tiles of all frames of a batch (see dbcdef.cu).
-__global__ void __launch_bounds__(kLrThreads, 4) restoration_batch_kernel(const LrArgs* __restrict__ frames,
-                                                                          const int* __restrict__ tile_prefix, int n,
-                                                                          int* queue) {
-    __shared__ int s_tile, s_frame;
-    __shared__ LrArgs s_args;
-    const int total = tile_prefix[n];
-    int have = -1;  // frame whose record s_args holds (uniform over the CTA)
-    // Thread 0 keeps the next tile index in hand: the atomic for tile k+1 is
-    // issued when tile k starts, so its latency hides behind tile k's work.
-    // A CTA takes tiles in increasing order, so the frame of a tile is found
-    // by stepping forward from the previous tile's frame.
-    int next = 0, frame = 0;
-    if (threadIdx.x == 0) next = atomicAdd(queue, 1);
-    for (;;) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const int t = next;
-            if (t < total) {
-                while (frame + 1 < n && tile_prefix[frame + 1] <= t) ++frame;
-                next = atomicAdd(queue, 1);
-            }
-            s_tile = t;
-            s_frame = frame;
-        }
-        __syncthreads();
-        const int t = s_tile;
-        if (t >= total) break;
-        const int f = s_frame;
-        if (f != have) {  // consecutive tiles mostly share a frame: copy its record once
-            have = f;
-            const int words = (int)(sizeof(LrArgs) / sizeof(int));
-            const int* src = reinterpret_cast<const int*>(frames + f);
-            int* dst = reinterpret_cast<int*>(&s_args);
-            for (int i = threadIdx.x; i < words; i += kLrThreads) dst[i] = src[i];
-            __syncthreads();
-        }
-        lr_tile(s_args, t - tile_prefix[f]);
-    }
+// Batched form: one CTA per tile of all frames of a batch (see dbcdef.cu).
+// MIN_CTAS picks the register budget: 4 resident CTAs per SM leave 64
+// registers a thread, 3 leave 80.
+template <int MIN_CTAS>
+__global__ void __launch_bounds__(kLrThreads, MIN_CTAS) restoration_batch_kernel(const LrArgs* __restrict__ frames,
+                                                                                const int* __restrict__ tile_prefix,
+                                                                                int n) {
+    const int f = frame_of_tile(tile_prefix, n, blockIdx.x);
+    lr_tile(frames[f], blockIdx.x - tile_prefix[f]);
 }
 
 // RestorationUnit::validate (restoration.rs:67-91).
@@ -687,7 +657,10 @@ cudaError_t lr_kernel_attributes() {
         cudaError_t e = cudaFuncSetAttribute(restoration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)kLrSmem);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(restoration_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            e = cudaFuncSetAttribute(restoration_batch_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kLrSmem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(restoration_batch_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)kLrSmem);
         if (e != cudaSuccess) return e;
         g_lr_attr_devices.fetch_or(1ull << dev, std::memory_order_release);
@@ -705,12 +678,16 @@ cudaError_t launch_restoration(const LrPlane* planes, int count, int bit_depth, 
     return launch_overlapped(restoration_kernel, dim3(total), dim3(kLrThreads), kLrSmem, stream, a);
 }
 
-cudaError_t launch_restoration_batch(const void* dev_args, const int* dev_prefix, int n, int* dev_queue, int grid,
+cudaError_t launch_restoration_batch(const void* dev_args, const int* dev_prefix, int n, int tiles, int ctas_per_sm,
                                      cudaStream_t stream) {
+    if (tiles <= 0) return cudaSuccess;
     cudaError_t e = lr_kernel_attributes();
     if (e != cudaSuccess) return e;
-    restoration_batch_kernel<<<grid, kLrThreads, kLrSmem, stream>>>(static_cast<const LrArgs*>(dev_args), dev_prefix,
-                                                                    n, dev_queue);
+    const LrArgs* args = static_cast<const LrArgs*>(dev_args);
+    if (ctas_per_sm <= 3)
+        restoration_batch_kernel<3><<<tiles, kLrThreads, kLrSmem, stream>>>(args, dev_prefix, n);
+    else
+        restoration_batch_kernel<4><<<tiles, kLrThreads, kLrSmem, stream>>>(args, dev_prefix, n);
     return cudaGetLastError();
 }
 
