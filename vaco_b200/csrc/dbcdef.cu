@@ -224,7 +224,8 @@ __device__ __forceinline__ void filter_line_class(int cls, uint16_t* q, int step
 // touch a common sample, so the lines run in place in any order.
 template <int PASS, int NT>
 __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem, int x0, int y0,
-                                             const SideWindow& side, uint32_t* s_list, int* s_count) {
+                                             const SideWindow& side, uint32_t* s_list, int* s_count,
+                                             const PairStrength* s_str) {
     const int tid = threadIdx.x;
     if (tid < 4) s_count[tid] = 0;
     __syncthreads();
@@ -314,14 +315,14 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
         if (PASS == 1 && ((first && h == 0) || (last && h == 1))) continue;
         const int lvl = e & 63, nq = (e >> 6) & 15, np = (e >> 10) & 15, off = (e >> 14) & 0x1FFF, p = (e >> 27) & 3;
         const int pitch = p ? gc.pitch : gl.pitch;
-        const Strength s = strength_of(lvl, a.sharpness);
         uint16_t* q = smem + a.plane_off[p] + off + (PASS == 0 ? 2 * h * pitch : 2 * h);
         const int reach = class_reach(cls);
         if (nq >= reach && np >= reach) {
-            filter_pair_class<PASS>(cls, q, pitch, pair_strength(s, a.bit_depth));
+            filter_pair_class<PASS>(cls, q, pitch, s_str[lvl], a.bit_depth - 8);
         } else {
             // near the plane edge: line by line, with clamped reads and
             // dropped writes
+            const Strength s = strength_of(lvl, a.sharpness);
             for (int l = 0; l < 2; ++l) {
                 if (PASS == 0)
                     filter_line_class<1>(cls, q + l * pitch, 1, nq, np, s, a.bit_depth);
@@ -344,6 +345,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     __shared__ PairBlock s_pair[3][64];
     __shared__ uint8_t s_active[64];
     __shared__ int s_count[4];
+    __shared__ PairStrength s_str[64];  // per loop-filter level, for this frame's sharpness and depth
     // The deblocking lists and side window are dead once deblocking is done;
     // the CDEF phase reuses their space for the odd-aligned luma pairs.
     __shared__ union {
@@ -479,8 +481,10 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
 
     // ---- deblocking, pass 0 (vertical edges) then pass 1 (horizontal edges)
     if (a.deblock_on) {
-        deblock_pass<0, NT>(a, smem, x0, y0, s_side, s_list, s_count);
-        deblock_pass<1, NT>(a, smem, x0, y0, s_side, s_list, s_count);
+        // visible to both passes after the first pass's opening barrier
+        if (tid < 64) s_str[tid] = pair_strength(strength_of(tid, a.sharpness), a.bit_depth - 8);
+        deblock_pass<0, NT>(a, smem, x0, y0, s_side, s_list, s_count, s_str);
+        deblock_pass<1, NT>(a, smem, x0, y0, s_side, s_list, s_count, s_str);
     }
 
     // ---- stripe-boundary rows of the deblocked picture for restoration:

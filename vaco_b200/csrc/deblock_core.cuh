@@ -339,15 +339,13 @@ __device__ __forceinline__ uint32_t sel2(uint32_t m, uint32_t a, uint32_t b) { r
 constexpr int kNarrowBias = 1 << 14;
 
 // Packed limit / blimit / thresh / flatness bound of a segment (7.14.4),
-// scaled to the bit depth.
-struct PairStrength {
+// scaled to the bit depth (sh = bit depth - 8).
+struct __align__(16) PairStrength {
     uint32_t limit, blimit, thresh, one;
-    int sh;
 };
 
-__device__ __forceinline__ PairStrength pair_strength(const Strength& s, int bd) {
-    const int sh = bd - 8;
-    return PairStrength{pk2(s.limit << sh), pk2(s.blimit << sh), pk2(s.thresh << sh), pk2(1 << sh), sh};
+__device__ __forceinline__ PairStrength pair_strength(const Strength& s, int sh) {
+    return PairStrength{pk2(s.limit << sh), pk2(s.blimit << sh), pk2(s.thresh << sh), pk2(1 << sh)};
 }
 
 // 2 |p0 - q0| + |p1 - q1| / 2, the blimit side of filterMask.
@@ -451,14 +449,14 @@ __device__ __forceinline__ void wide8_2(const uint32_t* P, const uint32_t* Q, ui
 
 // Filter size 4: mask over p1..q1, narrow filter.
 template <int PASS>
-__device__ __forceinline__ void pair_size4(uint16_t* q, int pitch, const PairStrength& s) {
+__device__ __forceinline__ void pair_size4(uint16_t* q, int pitch, const PairStrength& s, int sh) {
     uint32_t P[2], Q[2];
     load_pair<PASS, 2>(q, pitch, P, Q);
     const uint32_t dpq = pmax2(absd2(P[1], P[0]), absd2(Q[1], Q[0]));
     const uint32_t keep = mask2(over2(dpq, s.limit) | over2(blimit_term2(P, Q), s.blimit));
     if (keep == 0xFFFFFFFFu) return;
     uint32_t p1 = P[1], p0 = P[0], q0 = Q[0], q1 = Q[1];
-    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), s.sh);
+    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), sh);
     P[1] = sel2(keep, P[1], p1);
     P[0] = sel2(keep, P[0], p0);
     Q[0] = sel2(keep, Q[0], q0);
@@ -468,7 +466,7 @@ __device__ __forceinline__ void pair_size4(uint16_t* q, int pitch, const PairStr
 
 // Filter size 8 on a chroma plane (filter length 6).
 template <int PASS>
-__device__ __forceinline__ void pair_size6(uint16_t* q, int pitch, const PairStrength& s) {
+__device__ __forceinline__ void pair_size6(uint16_t* q, int pitch, const PairStrength& s, int sh) {
     uint32_t P[3], Q[3];
     load_pair<PASS, 3>(q, pitch, P, Q);
     const uint32_t dpq = pmax2(absd2(P[1], P[0]), absd2(Q[1], Q[0]));
@@ -477,7 +475,7 @@ __device__ __forceinline__ void pair_size6(uint16_t* q, int pitch, const PairStr
     if (keep == 0xFFFFFFFFu) return;
     const uint32_t steep = mask2(over2(pmax2(dpq, pmax2(absd2(P[2], P[0]), absd2(Q[2], Q[0]))), s.one));
     uint32_t p1 = P[1], p0 = P[0], q0 = Q[0], q1 = Q[1];
-    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), s.sh);
+    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), sh);
     if ((~steep & ~keep) != 0) {  // a flat line: the 6-tap filter
         const uint32_t p2 = P[2], q2 = Q[2], r = pk2(4), mk = 0x1FFF1FFFu;
         p1 = sel2(steep, p1, ((3u * p2 + 2u * P[1] + 2u * P[0] + Q[0] + r) >> 3) & mk);
@@ -508,14 +506,14 @@ __device__ __forceinline__ void masks8_2(const uint32_t* P, const uint32_t* Q, c
 
 // Filter size 8 on luma (filter length 8).
 template <int PASS>
-__device__ __forceinline__ void pair_size8(uint16_t* q, int pitch, const PairStrength& s) {
+__device__ __forceinline__ void pair_size8(uint16_t* q, int pitch, const PairStrength& s, int sh) {
     uint32_t P[4], Q[4];
     load_pair<PASS, 4>(q, pitch, P, Q);
     uint32_t dpq, keep, steep;
     masks8_2(P, Q, s, dpq, keep, steep);
     if (keep == 0xFFFFFFFFu) return;
     uint32_t p1 = P[1], p0 = P[0], q0 = Q[0], q1 = Q[1];
-    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), s.sh);
+    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), sh);
     const uint32_t n[4] = {p1, p0, q0, q1};
     if ((~steep & ~keep) == 0) {  // narrow lines only: samples -2 .. 1
 #pragma unroll
@@ -544,14 +542,14 @@ __device__ __forceinline__ void pair_size8(uint16_t* q, int pitch, const PairStr
 
 // Filter size 16 on luma: narrow, 8-tap or 14-tap by the flat masks.
 template <int PASS>
-__device__ __forceinline__ void pair_size16(uint16_t* q, int pitch, const PairStrength& s) {
+__device__ __forceinline__ void pair_size16(uint16_t* q, int pitch, const PairStrength& s, int sh) {
     uint32_t P[7], Q[7];
     load_pair<PASS, 7>(q, pitch, P, Q);
     uint32_t dpq, keep, steep;
     masks8_2(P, Q, s, dpq, keep, steep);
     if (keep == 0xFFFFFFFFu) return;
     uint32_t p1 = P[1], p0 = P[0], q0 = Q[0], q1 = Q[1];
-    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), s.sh);
+    narrow2(p1, p0, q0, q1, mask2(over2(dpq, s.thresh)), sh);
     const uint32_t n[4] = {p1, p0, q0, q1};
     const uint32_t flat = ~steep & ~keep, narrow = steep & ~keep;
     if (flat == 0) {  // narrow lines only: samples -2 .. 1
@@ -614,11 +612,11 @@ __device__ __forceinline__ void pair_size16(uint16_t* q, int pitch, const PairSt
 }
 
 template <int PASS>
-__device__ __forceinline__ void filter_pair_class(int cls, uint16_t* q, int pitch, const PairStrength& s) {
-    if (cls == 0) pair_size4<PASS>(q, pitch, s);
-    else if (cls == 1) pair_size6<PASS>(q, pitch, s);
-    else if (cls == 2) pair_size8<PASS>(q, pitch, s);
-    else pair_size16<PASS>(q, pitch, s);
+__device__ __forceinline__ void filter_pair_class(int cls, uint16_t* q, int pitch, const PairStrength& s, int sh) {
+    if (cls == 0) pair_size4<PASS>(q, pitch, s, sh);
+    else if (cls == 1) pair_size6<PASS>(q, pitch, s, sh);
+    else if (cls == 2) pair_size8<PASS>(q, pitch, s, sh);
+    else pair_size16<PASS>(q, pitch, s, sh);
 }
 
 // Samples per side a size class reads (and the per-line filters' clamping
