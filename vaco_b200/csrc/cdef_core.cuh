@@ -194,8 +194,9 @@ namespace cdefk {
 // subtracts never carry or borrow across lanes:
 //   hi = max(v, cur), lo = min(v, cur), |d| = hi - lo, d+ = hi - cur
 //   m  = t - min(|d| >> s, t)               (= max(0, t - (|d| >> s)))
-//   c  = min(|d|, m), c+ = min(c, d+), c- = c - c+   (constrain split by sign)
-//   acc+ / acc- += tap * c+ / c-            (each <= 24 * 240 = 5760)
+//   c  = min(|d|, m), c+ = min(c, d+)       (c+: constrain's positive part)
+//   acc+ += tap * c+, acc += tap * c        (each <= 24 * 240 = 5760), and
+//   at the end acc- = acc - acc+ (the negative parts' sum)
 // Output: with pos/neg the non-negative parts of acc+ - acc-,
 //   r+ = (pos + 8) >> 4, r- = (neg + 8) >> 4  (vaco's signed rounding)
 //   out = min(max(cur + r+, mn + r-) - r-, mx) = clamp(cur + r+ - r-, mn, mx).
@@ -264,7 +265,7 @@ __device__ __forceinline__ uint32_t load_pair(const WordTap& t, int word_off) { 
 
 template <bool MASK_MAX>
 __device__ __forceinline__ void pair_tap_step(uint32_t v, uint32_t cur, uint32_t t2, int s, uint32_t smask, uint32_t w,
-                                              uint32_t& accp, uint32_t& accn, uint32_t& mn, uint32_t& mx) {
+                                              uint32_t& accp, uint32_t& acct, uint32_t& mn, uint32_t& mx) {
     const uint32_t hi = vmax2(v, cur), lo = vmin2(v, cur);
     const uint32_t ad = hi - lo;
     const uint32_t sh = (ad >> s) & smask;
@@ -272,7 +273,7 @@ __device__ __forceinline__ void pair_tap_step(uint32_t v, uint32_t cur, uint32_t
     const uint32_t c = vmin2(ad, m);
     const uint32_t cp = vmin2(c, hi - cur);
     accp += w * cp;
-    accn += w * (c - cp);
+    acct += w * c;
     mn = vmin2(mn, v);
     mx = vmax2(mx, MASK_MAX ? (v & 0x3FFF3FFFu) : v);
 }
@@ -296,23 +297,24 @@ __device__ __forceinline__ uint32_t filter_pair(uint32_t cur, const Tap* taps, i
                                                 bool pri_on, bool sec_on) {
     const uint32_t tp = f.pri | ((uint32_t)f.pri << 16), ts = f.sec | ((uint32_t)f.sec << 16);
     const uint32_t pm = (0xFFFFu >> f.pri_shift) * 0x10001u, sm = (0xFFFFu >> f.sec_shift) * 0x10001u;
-    uint32_t accp = 0, accn = 0, mn = cur, mx = cur;
+    uint32_t accp = 0, acct = 0, mn = cur, mx = cur;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const uint32_t wp = k ? f.pt1 : f.pt0, ws = 2 - k;
         if (pri_on) {
-            pair_tap_step<MASK_MAX>(load_pair(taps[2 * k], row), cur, tp, f.pri_shift, pm, wp, accp, accn, mn, mx);
-            pair_tap_step<MASK_MAX>(load_pair(taps[2 * k + 1], row), cur, tp, f.pri_shift, pm, wp, accp, accn, mn, mx);
+            pair_tap_step<MASK_MAX>(load_pair(taps[2 * k], row), cur, tp, f.pri_shift, pm, wp, accp, acct, mn, mx);
+            pair_tap_step<MASK_MAX>(load_pair(taps[2 * k + 1], row), cur, tp, f.pri_shift, pm, wp, accp, acct, mn, mx);
         }
         if (sec_on) {
-            pair_tap_step<MASK_MAX>(load_pair(taps[4 + 2 * k], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn, mx);
-            pair_tap_step<MASK_MAX>(load_pair(taps[4 + 2 * k + 1], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn,
+            pair_tap_step<MASK_MAX>(load_pair(taps[4 + 2 * k], row), cur, ts, f.sec_shift, sm, ws, accp, acct, mn, mx);
+            pair_tap_step<MASK_MAX>(load_pair(taps[4 + 2 * k + 1], row), cur, ts, f.sec_shift, sm, ws, accp, acct, mn,
                                     mx);
-            pair_tap_step<MASK_MAX>(load_pair(taps[8 + 2 * k], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn, mx);
-            pair_tap_step<MASK_MAX>(load_pair(taps[8 + 2 * k + 1], row), cur, ts, f.sec_shift, sm, ws, accp, accn, mn,
+            pair_tap_step<MASK_MAX>(load_pair(taps[8 + 2 * k], row), cur, ts, f.sec_shift, sm, ws, accp, acct, mn, mx);
+            pair_tap_step<MASK_MAX>(load_pair(taps[8 + 2 * k + 1], row), cur, ts, f.sec_shift, sm, ws, accp, acct, mn,
                                     mx);
         }
     }
+    const uint32_t accn = acct - accp;
     const uint32_t both = vmin2(accp, accn);
     const uint32_t rp = ((accp - both + 0x00080008u) >> 4) & 0x0FFF0FFFu;
     const uint32_t rn = ((accn - both + 0x00080008u) >> 4) & 0x0FFF0FFFu;
