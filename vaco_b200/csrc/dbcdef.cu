@@ -211,24 +211,18 @@ __device__ __forceinline__ void filter_line_class(int cls, uint16_t* q, int step
     else line_size16<STEP>(q, step, nq, np, s, bd);
 }
 
-// One deblocking pass over the staged tiles of every plane (PASS 0: vertical
-// edges X = px0 + 4e, e <= tw/4, on 4-row cells from py0-8 (luma) or py0-4
-// (chroma); PASS 1: horizontal edges E = py0 + 4e, e <= th/4, on 4-column
-// cells from px0-4).  Each candidate segment gets its decision (7.14.2-7.14.5:
-// on screen, transform edge, filter size, level) and joins the list of its
-// size class.  The lines are then filtered in one loop over the class lists
-// laid end to end, 4 lanes per segment, so a warp changes filter code at most
-// at a class boundary.  The first and last cell of an edge contribute only
-// the lines the window needs: rows [py0-7, py0+th+7) / [py0-3, py0+th+3) in
-// pass 0, columns [px0-2, px0+tw+2) in pass 1.  Within a pass no two edges
-// touch a common sample, so the lines run in place in any order.
+// The edge segments of one deblocking pass over the staged tiles of every
+// plane (PASS 0: vertical edges X = px0 + 4e, e <= tw/4, on 4-row cells from
+// py0-8 (luma) or py0-4 (chroma); PASS 1: horizontal edges E = py0 + 4e,
+// e <= th/4, on 4-column cells from px0-4).  Each candidate segment gets its
+// decision (7.14.2-7.14.5: on screen, transform edge, filter size, level)
+// and joins the list of its size class.  The decisions read only the side
+// information, never samples, so both passes' lists are built in one phase
+// (s_count zeroed beforehand; the caller's barrier publishes the lists).
 template <int PASS, int NT>
-__device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem, int x0, int y0,
-                                             const SideWindow& side, uint32_t* s_list, int* s_count,
-                                             const PairStrength* s_str) {
+__device__ __forceinline__ void deblock_lists(const DbCdefArgs& a, int x0, int y0, const SideWindow& side,
+                                              uint32_t* s_list, int* s_count) {
     const int tid = threadIdx.x;
-    if (tid < 4) s_count[tid] = 0;
-    __syncthreads();
     const PlaneGeom gl = plane_geom(0, a.ssx, a.ssy), gc = plane_geom(1, a.ssx, a.ssy);
     const int na0 = PASS == 0 ? gl.th / 4 + 4 : gl.th / 4 + 1, nb0 = PASS == 0 ? gl.tw / 4 + 1 : gl.tw / 4 + 2;
     const int nac = PASS == 0 ? gc.th / 4 + 2 : gc.th / 4 + 1, nbc = PASS == 0 ? gc.tw / 4 + 1 : gc.tw / 4 + 2;
@@ -286,7 +280,19 @@ __device__ __forceinline__ void deblock_pass(const DbCdefArgs& a, uint16_t* smem
         s_list[c_list_off[cls] + at] =
             seg_entry(lvl, nq, np, off, p, PASS == 0 ? ia == 0 : ib == 0, PASS == 0 ? ia == na - 1 : ib == nb - 1);
     }
-    __syncthreads();
+}
+
+// The lines of one pass, filtered in one loop over its class lists laid end
+// to end, so a warp changes filter code at most at a class boundary.  The
+// first and last cell of an edge contribute only the lines the window needs:
+// rows [py0-7, py0+th+7) / [py0-3, py0+th+3) in pass 0, columns [px0-2,
+// px0+tw+2) in pass 1.  Within a pass no two edges touch a common sample, so
+// the lines run in place in any order.
+template <int PASS, int NT>
+__device__ __forceinline__ void deblock_filter(const DbCdefArgs& a, uint16_t* smem, const uint32_t* s_list,
+                                               const int* s_count, const PairStrength* s_str) {
+    const int tid = threadIdx.x;
+    const PlaneGeom gl = plane_geom(0, a.ssx, a.ssy), gc = plane_geom(1, a.ssx, a.ssy);
     // The lines, two per lane: lines 2h and 2h+1 of a segment (h = item & 1)
     // as the two halves of every register (filter_pair_class).  In pass 1
     // the first cell of an edge needs only its lines 2 and 3 and the last
@@ -344,13 +350,13 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     __shared__ int s_cost[64][8];
     __shared__ PairBlock s_pair[3][64];
     __shared__ uint8_t s_active[64];
-    __shared__ int s_count[4];
+    __shared__ int s_count[8];  // list lengths per size class, pass 0 then pass 1
     __shared__ PairStrength s_str[64];  // per loop-filter level, for this frame's sharpness and depth
     // The deblocking lists and side window are dead once deblocking is done;
     // the CDEF phase reuses their space for the odd-aligned luma pairs.
     __shared__ union {
         struct {
-            uint32_t list[kListTotal];  // per size class, see seg_entry()
+            uint32_t list[2 * kListTotal];  // per pass and size class, see seg_entry()
             SideWindow side;
         } db;
         uint32_t shifted[kShiftRows * (64 + 2 * kHalo) / 2];
@@ -377,6 +383,11 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         }
         s_active[tid] = act;
     }
+
+    // the deblocking lists' lengths and strengths, published by the staging
+    // barrier below
+    if (tid < 8) s_count[tid] = 0;
+    if (a.deblock_on && tid < 64) s_str[tid] = pair_strength(strength_of(tid, a.sharpness), a.bit_depth - 8);
 
     // ---- every plane's tile with an 8-sample halo (edge-clamped).  Whole
     // 16-byte chunks inside the plane go by cp.async, all in flight at once;
@@ -481,10 +492,11 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
 
     // ---- deblocking, pass 0 (vertical edges) then pass 1 (horizontal edges)
     if (a.deblock_on) {
-        // visible to both passes after the first pass's opening barrier
-        if (tid < 64) s_str[tid] = pair_strength(strength_of(tid, a.sharpness), a.bit_depth - 8);
-        deblock_pass<0, NT>(a, smem, x0, y0, s_side, s_list, s_count, s_str);
-        deblock_pass<1, NT>(a, smem, x0, y0, s_side, s_list, s_count, s_str);
+        deblock_lists<0, NT>(a, x0, y0, s_side, s_list, s_count);
+        deblock_lists<1, NT>(a, x0, y0, s_side, s_list + kListTotal, s_count + 4);
+        __syncthreads();
+        deblock_filter<0, NT>(a, smem, s_list, s_count, s_str);
+        deblock_filter<1, NT>(a, smem, s_list + kListTotal, s_count + 4, s_str);
     }
 
     // ---- stripe-boundary rows of the deblocked picture for restoration:
