@@ -107,6 +107,7 @@ struct DbCdefArgs {
     uint8_t y_pri[8], y_sec[8], uv_pri[8], uv_sec[8];
     DeviceStatus* status;
     int vec_ok;
+    int staged_vectors;         // 16-byte vectors of all staged planes together
     size_t plane_off[3];        // shared-memory offset (samples) of each staged plane
 };
 
@@ -367,7 +368,6 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int mi_r0 = tile_y * 16, mi_c0 = tile_x * 16;
     const int x0 = mi_c0 * 4, y0 = mi_r0 * 4;
-    const int maxv = (1 << a.bit_depth) - 1;
 
     // ---- CDEF block activity (decode.rs:772-779)
     const long slot = (long)(mi_r0 >> 4) * a.cdef_stride + (mi_c0 >> 4);
@@ -466,28 +466,18 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         if (bad) report_error(a.status, STAGE_DEBLOCK, 0, VACO_AV1_MSG_DB_PARAMS);
     }
     {
+        // Every staged sample, halo included: the halo holds samples of the
+        // same planes (edge-clamped copies past their borders), so the tiles
+        // together check exactly the planes' samples, and a flat pass over
+        // the staged vectors needs no per-row indexing.
         const uint32_t hi = ((0xFFFFu << a.bit_depth) & 0xFFFFu) * 0x10001u;  // bits above the depth, per lane
-        int bad = 0;
-        for (int p = 0; p < a.num_planes; ++p) {
-            const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
-            const DevPlaneC& P = a.src[p];
-            const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
-            const int cpr = g.tw / 8, rows = min(g.th, P.height - py0);
-            const uint16_t* t = smem + a.plane_off[p];
-            for (int v = tid; v < rows * cpr; v += NT) {
-                const int r = v >> (3 - g.sx), cv = v - r * cpr;  // cpr = tw / 8 = 8 >> sx
-                const int x = px0 + cv * 8;
-                if (x >= P.width) continue;
-                const uint16_t* q = t + (r + kHalo) * g.pitch + kHalo + cv * 8;
-                if (x + 8 <= P.width) {
-                    const uint4 w = *reinterpret_cast<const uint4*>(q);
-                    bad |= ((w.x | w.y | w.z | w.w) & hi) != 0;
-                } else {
-                    for (int k = 0; k < P.width - x; ++k) bad |= q[k] > maxv;
-                }
-            }
+        const uint4* v = reinterpret_cast<const uint4*>(smem);
+        uint32_t acc = 0;
+        for (int i = tid; i < a.staged_vectors; i += NT) {
+            const uint4 w = v[i];
+            acc |= w.x | w.y | w.z | w.w;
         }
-        if (bad) report_error(a.status, STAGE_DEBLOCK, 1, VACO_AV1_MSG_DB_SAMPLE);
+        if (acc & hi) report_error(a.status, STAGE_DEBLOCK, 1, VACO_AV1_MSG_DB_SAMPLE);
     }
 
     // ---- deblocking, pass 0 (vertical edges) then pass 1 (horizontal edges)
@@ -648,12 +638,12 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     }
 }
 
-// NT threads per tile, MIN_CTAS CTAs per SM.  With 256 threads, 3 CTAs
-// leave 80 registers a thread (fewer instructions and instruction-fetch
-// stalls, 1 % faster on a 4K frame) and 4 fill more SMs at once, which wins
-// when a frame has few tiles (a 1080p frame's 510 tiles fit one wave of 4 per
-// SM; at 3 per SM they take two).  128 threads at 5 CTAs per SM is the
-// smaller-CTA shape: shorter barriers, about the same warps per SM.
+// NT threads per tile, MIN_CTAS CTAs per SM.  The per-frame path runs 256
+// threads at 4 CTAs per SM (64 registers a thread), measured at least as fast
+// as 3 (80 registers) on 1080p and on 2560-, 2880- and 3840-wide frames
+// (1.5-2 % faster on the last two); 128 threads at 5 CTAs
+// per SM is the smaller-CTA shape (shorter barriers, about the same warps per
+// SM).  The batched form also has the 256 x 3 body (see dbcdef_batch_kernel).
 template <int NT, int MIN_CTAS>
 __global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_kernel(DbCdefArgs a) {
     overlap_prologue();
@@ -731,14 +721,14 @@ size_t build_dbcdef_args(const DbCdefLaunch& L, void* out) {
     }
     a.status = L.status;
     a.vec_ok = vec;
+    a.staged_vectors = (int)(off / 8);  // each staged plane is a multiple of 8 samples
     memcpy(out, &a, sizeof a);
     return off * sizeof(uint16_t);
 }
 
-// Per-device caches, shared by every host thread that launches: atomics, so
+// Per-device cache, shared by every host thread that launches: an atomic, so
 // concurrent first launches on a device only repeat idempotent set-up.
 std::atomic<unsigned long long> g_attr_devices{0};
-std::atomic<int> g_sm_counts[64];
 
 cudaError_t dbcdef_kernel_attributes() {
     int dev = 0;
@@ -746,8 +736,7 @@ cudaError_t dbcdef_kernel_attributes() {
     if (dev < 64 && !(g_attr_devices.load(std::memory_order_acquire) & (1ull << dev))) {
         constexpr int kMaxSmem = 96 * 1024;
         const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-        cudaError_t e = cudaFuncSetAttribute(dbcdef_kernel<256, 3>, attr, kMaxSmem);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_kernel<256, 4>, attr, kMaxSmem);
+        cudaError_t e = cudaFuncSetAttribute(dbcdef_kernel<256, 4>, attr, kMaxSmem);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_kernel<128, 5>, attr, kMaxSmem);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<256, 3>, attr, kMaxSmem);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<256, 4>, attr, kMaxSmem);
@@ -765,19 +754,6 @@ cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
     if (e != cudaSuccess) return e;
     dim3 grid(div_up(L.info.mi_cols, 16), div_up(L.info.mi_rows, 16));
     if (L.threads == 128) return launch_overlapped(dbcdef_kernel<128, 5>, grid, dim3(128), smem, stream, a);
-    // 256 threads: 3 CTAs per SM once the frame has more than 2.5 waves of 4
-    // per SM (measured best on 4K and 2880-wide frames; 4 on 1080p and
-    // 2560-wide).
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64) {
-        int n = g_sm_counts[dev].load(std::memory_order_relaxed);
-        if (n <= 0 && cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0)
-            g_sm_counts[dev].store(n, std::memory_order_relaxed);
-        if (n > 0) sms = n;
-    }
-    if ((long)grid.x * grid.y * 2 > 5L * 4 * sms)
-        return launch_overlapped(dbcdef_kernel<256, 3>, grid, dim3(256), smem, stream, a);
     return launch_overlapped(dbcdef_kernel<256, 4>, grid, dim3(256), smem, stream, a);
 }
 
