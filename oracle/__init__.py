@@ -170,7 +170,7 @@ def restore_plane(before: np.ndarray, after: np.ndarray, width: int, height: int
 # ---------------------------------------------------------------- deblocking
 def deblock_picture(f: FrameInputs, threads: int | None = None):
     """AV1 7.14 loop filter (spec restatement; no vaco counterpart)."""
-    planes = [_u16(p) for p in f.planes]
+    planes = [_u16(p) for p in f.planes[: f.num_planes]]
     outs = [np.zeros_like(p) for p in planes]
     shapes = [p.shape for p in planes]
     src = picture_struct([ptr(p) for p in planes], shapes)

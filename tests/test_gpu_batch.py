@@ -38,6 +38,25 @@ def test_batch_matches_oracle_frame_by_frame(ctx, graphs, largest_first, oracle_
             np.testing.assert_array_equal(g, w)
 
 
+def test_batch_mixed_chroma_layouts_match_oracle(ctx, oracle_threads):
+    """One batch of 4:2:0, 4:2:2, 4:4:4 and monochrome frames: the batched
+    fused kernel reads each frame's layout from its record."""
+    layouts = [((1, 1), False), ((1, 0), False), ((0, 0), False), ((1, 1), True)]
+    geoms = [(200, 136, 10, None), (328, 200, 10, 400), (60, 44, 8, None), (520, 264, 12, None),
+             (120, 72, 8, 136), (96, 80, 12, None), (204, 130, 8, None), (256, 128, 10, 320)]
+    frames = [synth.make_small(700 + i, w, h, bd, upscaled_width=up, sharpness=None, with_lvl_map=i % 2 == 0,
+                               subsampling=sub, monochrome=mono)
+              for i, ((sub, mono), (w, h, bd, up)) in enumerate(zip(layouts * 2, geoms))]
+    devs = [DeviceFrame(f) for f in frames]
+    st, ms = ctx.postfilter_batch_dev(devs, stream=torch.cuda.current_stream().cuda_stream)
+    assert st == [0] * len(frames) and ms == [0] * len(frames)
+    for i, (f, d) in enumerate(zip(frames, devs)):
+        want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+        assert m == 0
+        for k, (g, w) in enumerate(zip(d.outputs_numpy(), want)):
+            assert np.array_equal(g, w), f"frame {i} layout {layouts[i % 4]} plane {k} differs"
+
+
 def test_batch_graph_replay_with_new_data(ctx, oracle_threads):
     ctx.set_tuning(use_graphs=1)
     stream = torch.cuda.current_stream().cuda_stream

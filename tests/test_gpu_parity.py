@@ -133,6 +133,52 @@ def test_postfilter_chain_small(ctx, geom, oracle_threads):
         assert_planes_equal(ctx.postfilter_frame(f), want, f"chain seed={seed}")
 
 
+LAYOUTS = [((1, 0), False), ((0, 0), False), ((1, 1), True)]
+LAYOUT_IDS = ["422", "444", "mono"]
+
+
+@pytest.mark.parametrize("layout", LAYOUTS, ids=LAYOUT_IDS)
+@pytest.mark.parametrize("geom", [(200, 136, 10, None), (60, 44, 8, None), (100, 58, 12, 124), (520, 264, 10, None)])
+def test_postfilter_chain_layouts(ctx, layout, geom, oracle_threads):
+    """4:2:2, 4:4:4 and monochrome frames through the whole chain, through
+    the host and the device entry points."""
+    w, h, bd, up = geom
+    sub, mono = layout
+    for seed, lvl_map in ((21, False), (22, True)):
+        f = synth.make_small(seed, w, h, bd, upscaled_width=up, sharpness=None, with_lvl_map=lvl_map,
+                             subsampling=sub, monochrome=mono)
+        want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+        assert m == 0
+        assert_planes_equal(ctx.postfilter_frame(f), want, f"chain {layout} seed={seed}")
+        d = DeviceFrame(f)
+        ctx.postfilter_frame_dev(d)
+        assert_planes_equal(d.outputs_numpy(), want, f"chain dev {layout} seed={seed}")
+
+
+@pytest.mark.parametrize("layout", LAYOUTS, ids=LAYOUT_IDS)
+def test_cdef_and_deblock_layouts(ctx, layout, oracle_threads):
+    """The standalone CDEF and deblocking entry points on the same layouts."""
+    sub, mono = layout
+    for seed, (w, h, bd) in enumerate([(200, 136, 10), (60, 44, 8), (96, 80, 12)]):
+        f = synth.make_small(30 + seed, w, h, bd, sharpness=None, with_lvl_map=seed == 1, subsampling=sub,
+                             monochrome=mono)
+        want, m = oracle.cdef_picture(f, threads=oracle_threads)
+        assert m == 0
+        assert_planes_equal(ctx.cdef_picture(f), want, f"cdef {layout}")
+        want, m = oracle.deblock_picture(f, threads=oracle_threads)
+        assert m == 0
+        assert_planes_equal(ctx.deblock_picture(f), want, f"deblock {layout}")
+
+
+def test_postfilter_chain_444_1080p(ctx, oracle_threads):
+    """A full-size 4:4:4 frame: every plane takes the 64x64 tile layout."""
+    f = synth.make_frame(synth.Workload("chain_1080p_444", 1920, 1080, 10, 1920, True), synth.seed_for(9, 4),
+                         subsampling=(0, 0))
+    want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+    assert m == 0
+    assert_planes_equal(ctx.postfilter_frame(f), want, "chain 1080p 4:4:4")
+
+
 @pytest.mark.parametrize("workload", [synth.CONFIG1, synth.CONFIG2, synth.CONFIG2_DENOM12, synth.CONFIG0],
                          ids=lambda w: w.name)
 def test_postfilter_chain_full_size(ctx, workload, oracle_threads):

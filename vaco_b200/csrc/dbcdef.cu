@@ -221,10 +221,10 @@ __device__ __forceinline__ void filter_line_class(int cls, uint16_t* q, int step
 // information, never samples, so both passes' lists are built in one phase
 // (s_count zeroed beforehand; the caller's barrier publishes the lists).
 template <int PASS, int NT>
-__device__ __forceinline__ void deblock_lists(const DbCdefArgs& a, int x0, int y0, const SideWindow& side,
-                                              uint32_t* s_list, int* s_count) {
+__device__ __forceinline__ void deblock_lists(const DbCdefArgs& a, int ssx, int ssy, int x0, int y0,
+                                              const SideWindow& side, uint32_t* s_list, int* s_count) {
     const int tid = threadIdx.x;
-    const PlaneGeom gl = plane_geom(0, a.ssx, a.ssy), gc = plane_geom(1, a.ssx, a.ssy);
+    const PlaneGeom gl = plane_geom(0, ssx, ssy), gc = plane_geom(1, ssx, ssy);
     const int na0 = PASS == 0 ? gl.th / 4 + 4 : gl.th / 4 + 1, nb0 = PASS == 0 ? gl.tw / 4 + 1 : gl.tw / 4 + 2;
     const int nac = PASS == 0 ? gc.th / 4 + 2 : gc.th / 4 + 1, nbc = PASS == 0 ? gc.tw / 4 + 1 : gc.tw / 4 + 2;
     const int n0 = na0 * nb0, nc = a.num_planes > 1 ? nac * nbc : 0;
@@ -290,10 +290,11 @@ __device__ __forceinline__ void deblock_lists(const DbCdefArgs& a, int x0, int y
 // px0+tw+2) in pass 1.  Within a pass no two edges touch a common sample, so
 // the lines run in place in any order.
 template <int PASS, int NT>
-__device__ __forceinline__ void deblock_filter(const DbCdefArgs& a, uint16_t* smem, const uint32_t* s_list,
-                                               const int* s_count, const PairStrength* s_str) {
+__device__ __forceinline__ void deblock_filter(const DbCdefArgs& a, int ssx, int ssy, uint16_t* smem,
+                                               const uint32_t* s_list, const int* s_count,
+                                               const PairStrength* s_str) {
     const int tid = threadIdx.x;
-    const PlaneGeom gl = plane_geom(0, a.ssx, a.ssy), gc = plane_geom(1, a.ssx, a.ssy);
+    const PlaneGeom gl = plane_geom(0, ssx, ssy), gc = plane_geom(1, ssx, ssy);
     // The lines, two per lane: lines 2h and 2h+1 of a segment (h = item & 1)
     // as the two halves of every register (filter_pair_class).  In pass 1
     // the first cell of an edge needs only its lines 2 and 3 and the last
@@ -344,9 +345,12 @@ __device__ __forceinline__ void deblock_filter(const DbCdefArgs& a, uint16_t* sm
 // One 64x64 filter block (tile_x, tile_y) of one frame.  Every thread of the
 // CTA calls it; it ends with all threads past their last shared-memory use
 // only after the caller's next __syncthreads().
-template <int NT>
+template <int NT, int LAYOUT>
 __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int tile_y) {
     constexpr int kWarpsNT = NT / 32;
+    // chroma subsampling: LAYOUT = ssx | ssy << 1 fixes it at compile time
+    // (every plane geometry below becomes a constant); LAYOUT < 0 reads it
+    const int ssx = LAYOUT < 0 ? a.ssx : (LAYOUT & 1), ssy = LAYOUT < 0 ? a.ssy : (LAYOUT >> 1);
     extern __shared__ __align__(16) uint16_t smem[];
     __shared__ int s_cost[64][8];
     __shared__ PairBlock s_pair[3][64];
@@ -396,7 +400,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     // interior tiles with 2-D tensor copies instead measured 1.4 % slower
     // for the whole chain: the extra path costs more than the copies save.)
     for (int p = 0; p < a.num_planes; ++p) {
-        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        const PlaneGeom g = plane_geom(p, ssx, ssy);
         const DevPlaneC& P = a.src[p];
         uint16_t* t = smem + a.plane_off[p];
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
@@ -422,8 +426,8 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     // ---- the side information the deblocking decisions read, while the
     // copies are in flight (cells the two passes touch; see SideWindow)
     {
-        const int crows = (a.mi_rows + a.ssy) >> a.ssy, ccols = (a.mi_cols + a.ssx) >> a.ssx;
-        const int cr0 = (mi_r0 >> a.ssy) - kWinTop, cc0 = (mi_c0 >> a.ssx) - kWinLeft;
+        const int crows = (a.mi_rows + ssy) >> ssy, ccols = (a.mi_cols + ssx) >> ssx;
+        const int cr0 = (mi_r0 >> ssy) - kWinTop, cc0 = (mi_c0 >> ssx) - kWinLeft;
         for (int i = tid; i < kWinCells; i += NT) {
             const int wr = i / kWinCols, wc = i - wr * kWinCols;
             const int r = mi_r0 - kWinTop + wr, c = mi_c0 - kWinLeft + wc;
@@ -455,11 +459,11 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
             }
         }
         if (a.num_planes > 1) {
-            const int ccols = (a.mi_cols + a.ssx) >> a.ssx, crows = (a.mi_rows + a.ssy) >> a.ssy;
-            const int cw = 16 >> a.ssx, ch = 16 >> a.ssy;
+            const int ccols = (a.mi_cols + ssx) >> ssx, crows = (a.mi_rows + ssy) >> ssy;
+            const int cw = 16 >> ssx, ch = 16 >> ssy;
             for (int i = tid; i < cw * ch; i += NT) {
-                const int dr = i >> (4 - a.ssx), dc = i - dr * cw;  // cw = 16 >> ssx
-                const int r = (mi_r0 >> a.ssy) + dr, c = (mi_c0 >> a.ssx) + dc;
+                const int dr = i >> (4 - ssx), dc = i - dr * cw;  // cw = 16 >> ssx
+                const int r = (mi_r0 >> ssy) + dr, c = (mi_c0 >> ssx) + dc;
                 if (r < crows && c < ccols) bad |= s_side.tx[1][(dr + kWinTop) * kWinCols + dc + kWinLeft] > 18;
             }
         }
@@ -482,11 +486,11 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
 
     // ---- deblocking, pass 0 (vertical edges) then pass 1 (horizontal edges)
     if (a.deblock_on) {
-        deblock_lists<0, NT>(a, x0, y0, s_side, s_list, s_count);
-        deblock_lists<1, NT>(a, x0, y0, s_side, s_list + kListTotal, s_count + 4);
+        deblock_lists<0, NT>(a, ssx, ssy, x0, y0, s_side, s_list, s_count);
+        deblock_lists<1, NT>(a, ssx, ssy, x0, y0, s_side, s_list + kListTotal, s_count + 4);
         __syncthreads();
-        deblock_filter<0, NT>(a, smem, s_list, s_count, s_str);
-        deblock_filter<1, NT>(a, smem, s_list + kListTotal, s_count + 4, s_str);
+        deblock_filter<0, NT>(a, ssx, ssy, smem, s_list, s_count, s_str);
+        deblock_filter<1, NT>(a, ssx, ssy, smem, s_list + kListTotal, s_count + 4, s_str);
     }
 
     // ---- stripe-boundary rows of the deblocked picture for restoration:
@@ -495,7 +499,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     for (int p = 0; p < a.num_planes; ++p) {
         const DevPlane& R = a.pre_rows[p];
         if (!R.data) continue;
-        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        const PlaneGeom g = plane_geom(p, ssx, ssy);
         const int sh = 64 >> g.sy, off = 8 >> g.sy;
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
         const uint16_t* src = smem + a.plane_off[p];
@@ -518,7 +522,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     if (!any_active) {
         // Nothing filtered (or CDEF off): the output is the deblocked tile.
         for (int p = 0; p < a.num_planes; ++p) {
-            const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+            const PlaneGeom g = plane_geom(p, ssx, ssy);
             const DevPlane& d = a.dst[p];
             const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
             const uint16_t* t = smem + a.plane_off[p];
@@ -533,7 +537,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     }
     // Samples outside the plane become the "unavailable" sentinel for CDEF.
     for (int p = 0; p < a.num_planes; ++p) {
-        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        const PlaneGeom g = plane_geom(p, ssx, ssy);
         const DevPlane& d = a.dst[p];
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
         if (px0 + g.tw + 2 <= d.width && py0 + g.th + 2 <= d.height && px0 >= 2 && py0 >= 2) continue;
@@ -592,7 +596,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         }
         int primary = (sp << a.shift) & 0xFFFF;
         const int secondary = (ss << a.shift) & 0xFFFF;
-        const int chosen = primary == 0 ? 0 : chroma ? chroma_direction(dir, a.ssx, a.ssy) : dir;
+        const int chosen = primary == 0 ? 0 : chroma ? chroma_direction(dir, ssx, ssy) : dir;
         if (!chroma) primary = adjust_strength(primary, var);
         const int damping = (a.damping + a.shift - (chroma ? 1 : 0)) & 0xFF;
         // Each plane reports its own failure; the status word keeps the
@@ -602,7 +606,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
             report_error(a.status, STAGE_CDEF, ((unsigned long long)r * a.mi_cols + c) * 4 + 1 + p,
                          index >= 8 ? VACO_AV1_MSG_CDEF_STRENGTH_INDEX : VACO_AV1_MSG_CDEF_BLOCK_PARAMS);
         }
-        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        const PlaneGeom g = plane_geom(p, ssx, ssy);
         s_pair[p][b] = make_pair_block(chosen, primary, secondary, min(damping, 12), a.shift, g.pitch);
     }
     __syncthreads();
@@ -610,7 +614,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
     // Filtering: pixel pairs (two 16-bit lanes per register), one warp per
     // block row, lanes across the tile width.
     for (int p = 0; p < a.num_planes; ++p) {
-        const PlaneGeom g = plane_geom(p, a.ssx, a.ssy);
+        const PlaneGeom g = plane_geom(p, ssx, ssy);
         const DevPlane& d = a.dst[p];
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
         const bool edge = px0 < 2 || py0 < 2 || px0 + g.tw + 2 > d.width || py0 + g.th + 2 > d.height;
@@ -644,10 +648,10 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
 // (1.5-2 % faster on the last two); 128 threads at 5 CTAs
 // per SM is the smaller-CTA shape (shorter barriers, about the same warps per
 // SM).  The batched form also has the 256 x 3 body (see dbcdef_batch_kernel).
-template <int NT, int MIN_CTAS>
+template <int NT, int MIN_CTAS, int LAYOUT>
 __global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_kernel(DbCdefArgs a) {
     overlap_prologue();
-    dbcdef_tile<NT>(a, blockIdx.x, blockIdx.y);
+    dbcdef_tile<NT, LAYOUT>(a, blockIdx.x, blockIdx.y);
 }
 
 // Batched form: one CTA per tile of all frames of a batch, frames laid end to
@@ -663,7 +667,7 @@ __global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_batch_kernel(const DbCdef
     const DbCdefArgs& a = frames[f];
     const int local = blockIdx.x - tile_prefix[f];
     const int tiles_x = (a.mi_cols + 15) / 16;
-    dbcdef_tile<NT>(a, local % tiles_x, local / tiles_x);
+    dbcdef_tile<NT, -1>(a, local % tiles_x, local / tiles_x);
 }
 
 }  // namespace
@@ -736,8 +740,10 @@ cudaError_t dbcdef_kernel_attributes() {
     if (dev < 64 && !(g_attr_devices.load(std::memory_order_acquire) & (1ull << dev))) {
         constexpr int kMaxSmem = 96 * 1024;
         const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-        cudaError_t e = cudaFuncSetAttribute(dbcdef_kernel<256, 4>, attr, kMaxSmem);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_kernel<128, 5>, attr, kMaxSmem);
+        cudaError_t e = cudaSuccess;
+        for (auto k : {dbcdef_kernel<256, 4, 0>, dbcdef_kernel<256, 4, 1>, dbcdef_kernel<256, 4, 3>,
+                       dbcdef_kernel<128, 5, 0>, dbcdef_kernel<128, 5, 1>, dbcdef_kernel<128, 5, 3>})
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k, attr, kMaxSmem);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<256, 3>, attr, kMaxSmem);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<256, 4>, attr, kMaxSmem);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<128, 5>, attr, kMaxSmem);
@@ -753,8 +759,14 @@ cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
     cudaError_t e = dbcdef_kernel_attributes();
     if (e != cudaSuccess) return e;
     dim3 grid(div_up(L.info.mi_cols, 16), div_up(L.info.mi_rows, 16));
-    if (L.threads == 128) return launch_overlapped(dbcdef_kernel<128, 5>, grid, dim3(128), smem, stream, a);
-    return launch_overlapped(dbcdef_kernel<256, 4>, grid, dim3(256), smem, stream, a);
+    // one kernel per chroma layout (4:4:4 and monochrome, 4:2:2, 4:2:0)
+    const int layout = a.ssx | a.ssy << 1;
+    if (L.threads == 128) {
+        auto k = layout == 3 ? dbcdef_kernel<128, 5, 3> : layout == 1 ? dbcdef_kernel<128, 5, 1> : dbcdef_kernel<128, 5, 0>;
+        return launch_overlapped(k, grid, dim3(128), smem, stream, a);
+    }
+    auto k = layout == 3 ? dbcdef_kernel<256, 4, 3> : layout == 1 ? dbcdef_kernel<256, 4, 1> : dbcdef_kernel<256, 4, 0>;
+    return launch_overlapped(k, grid, dim3(256), smem, stream, a);
 }
 
 cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int n, int tiles, size_t smem,

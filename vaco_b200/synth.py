@@ -182,15 +182,19 @@ def cdef_settings(rng) -> CdefSettings:
 
 
 def make_frame(w: Workload, seed: int, *, sharpness: Optional[int] = 0, with_lvl_map: bool = False,
-               lr_unit: int = 64) -> FrameInputs:
+               lr_unit: int = 64, subsampling=(1, 1), monochrome: bool = False) -> FrameInputs:
+    """A seeded frame.  subsampling = (x, y): (1, 1) 4:2:0, (1, 0) 4:2:2,
+    (0, 0) 4:4:4; monochrome keeps luma only (the chroma planes are still
+    drawn, so the luma content matches the 4:2:0 frame of the same seed)."""
     rng = np.random.Generator(np.random.PCG64(seed))
+    ssx, ssy = subsampling
     mi_cols = 2 * ((w.width + 7) >> 3)
     mi_rows = 2 * ((w.height + 7) >> 3)
     planes: List[np.ndarray] = []
     for k in range(3):
-        s = 1 if k else 0
-        planes.append(content_plane(rng, (mi_rows * 4) >> s, (mi_cols * 4) >> s, w.bit_depth))
-    tx_l, tx_c = tx_maps(rng, mi_rows, mi_cols)
+        sx, sy = (ssx, ssy) if k else (0, 0)
+        planes.append(content_plane(rng, (mi_rows * 4) >> sy, (mi_cols * 4) >> sx, w.bit_depth))
+    tx_l, tx_c = tx_maps(rng, mi_rows, mi_cols, ssx, ssy)
     # 20% of 8x8 blocks skipped (all four 4x4 cells)
     skip8 = (rng.random(((mi_rows + 1) // 2, (mi_cols + 1) // 2)) < 0.2).astype(np.uint8)
     skip = np.repeat(np.repeat(skip8, 2, 0), 2, 1)[:mi_rows, :mi_cols].copy()
@@ -211,6 +215,7 @@ def make_frame(w: Workload, seed: int, *, sharpness: Optional[int] = 0, with_lvl
         bit_depth=w.bit_depth, coded_width=w.width, coded_height=w.height,
         upscaled_width=w.upscaled_width, planes=planes, tx_luma=tx_l, tx_chroma=tx_c,
         skip=skip, cdef_idx=idx, lvl_map=lvl_map, sharpness=sharpness, cdef=cdef,
+        subsampling_x=ssx, subsampling_y=ssy, monochrome=monochrome,
     )
     if w.chain:
         f.deblock_levels = levels
@@ -219,7 +224,9 @@ def make_frame(w: Workload, seed: int, *, sharpness: Optional[int] = 0, with_lvl
         f.lr_units = []
         for k in range(3):
             rows, cols = f.output_shape(k)
-            f.lr_units.append(lr_units(rng, cols, rows, lr_unit, k > 0))
+            units = lr_units(rng, cols, rows, lr_unit, k > 0)
+            if k < f.num_planes:
+                f.lr_units.append(units)
     else:
         f.deblock_levels = (0, 0, 0, 0)
         f.lr_type = (abi.FRAME_LR_NONE,) * 3
