@@ -212,23 +212,29 @@ __device__ __forceinline__ void filter_line_class(int cls, uint16_t* q, int step
     else line_size16<STEP>(q, step, nq, np, s, bd);
 }
 
-// The edge segments of one deblocking pass over the staged tiles of every
-// plane (PASS 0: vertical edges X = px0 + 4e, e <= tw/4, on 4-row cells from
-// py0-8 (luma) or py0-4 (chroma); PASS 1: horizontal edges E = py0 + 4e,
-// e <= th/4, on 4-column cells from px0-4).  Each candidate segment gets its
-// decision (7.14.2-7.14.5: on screen, transform edge, filter size, level)
-// and joins the list of its size class.  The decisions read only the side
-// information, never samples, so both passes' lists are built in one phase
-// (s_count zeroed beforehand; the caller's barrier publishes the lists).
-template <int PASS, int NT>
+// The edge segments of both deblocking passes over the staged tiles of every
+// plane, cell by cell.  A cell is a 4x4 block of samples at (xp, yp) =
+// (px0 - 4 + 4 cc, py0 - 4 top + 4 cr), top = 2 (luma) or 1 (chroma), on
+// (th/4 + 2 top) x (tw/4 + 2) cells.  Its left side is a candidate segment
+// of pass 0 (vertical edges X = px0 + 4e, e <= tw/4, on rows from py0-8 or
+// py0-4) and its top side one of pass 1 (horizontal edges E = py0 + 4e,
+// e <= th/4, on columns from px0-4); the two share the cell's position
+// checks, transform size and level word.  Each candidate gets its decision
+// (7.14.2-7.14.5: on screen, transform edge, filter size, level) and joins
+// its pass's list of its size class: pass 0 at s_list / s_count, pass 1 at
+// s_list + kListTotal / s_count + 4.  The decisions read only the side
+// information, never samples (s_count zeroed beforehand; the caller's
+// barrier publishes the lists).
+template <int NT>
 __device__ __forceinline__ void deblock_lists(const DbCdefArgs& a, int ssx, int ssy, int x0, int y0,
                                               const SideWindow& side, uint32_t* s_list, int* s_count) {
     const int tid = threadIdx.x;
     const PlaneGeom gl = plane_geom(0, ssx, ssy), gc = plane_geom(1, ssx, ssy);
-    const int na0 = PASS == 0 ? gl.th / 4 + 4 : gl.th / 4 + 1, nb0 = PASS == 0 ? gl.tw / 4 + 1 : gl.tw / 4 + 2;
-    const int nac = PASS == 0 ? gc.th / 4 + 2 : gc.th / 4 + 1, nbc = PASS == 0 ? gc.tw / 4 + 1 : gc.tw / 4 + 2;
-    const int n0 = na0 * nb0, nc = a.num_planes > 1 ? nac * nbc : 0;
-    const unsigned m0 = small_div_magic(nb0), mc = small_div_magic(nbc);
+    const int nrl = gl.th / 4 + 4, ncl = gl.tw / 4 + 2;  // luma cells: rows, columns
+    const int nrc = gc.th / 4 + 2, ncc = gc.tw / 4 + 2;  // chroma
+    const int n0 = nrl * ncl, nc = a.num_planes > 1 ? nrc * ncc : 0;
+    const unsigned m0 = small_div_magic(ncl), mc = small_div_magic(ncc);
+    const int mi_r0 = y0 >> 2, mi_c0 = x0 >> 2;
     for (int i = tid; i < n0 + 2 * nc; i += NT) {
         int p = 0, j = i;
         if (j >= n0) {
@@ -241,45 +247,64 @@ __device__ __forceinline__ void deblock_lists(const DbCdefArgs& a, int ssx, int 
         }
         if (p != 0 && a.levels[1 + p] == 0) continue;
         const PlaneGeom g = p ? gc : gl;
-        const int na = p ? nac : na0, nb = p ? nbc : nb0;
-        const int ia = small_div(j, p ? mc : m0), ib = j - ia * nb;
+        const int nr = p ? nrc : nrl, ncol = p ? ncc : ncl, top = p ? 1 : 2;
+        const int cr = small_div(j, p ? mc : m0), cc = j - cr * ncol;
         const DevPlane& P = a.dst[p];
         const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
-        const int yp = PASS == 0 ? py0 - (p ? 4 : 8) + 4 * ia : py0 + 4 * ia;
-        const int xp = PASS == 0 ? px0 + 4 * ib : px0 - 4 + 4 * ib;
+        const int yp = py0 + 4 * (cr - top), xp = px0 - 4 + 4 * cc;
         const int col = (xp >> 2) << g.sx, row = (yp >> 2) << g.sy;
-        const bool on_screen = xp >= 0 && yp >= 0 && xp < P.width && yp < P.height && col * 4 < a.coded_width &&
-                               row * 4 < a.coded_height && (PASS == 0 ? xp > 0 : yp > 0);
-        if (!on_screen) continue;
+        if (!(xp >= 0 && yp >= 0 && xp < P.width && yp < P.height && col * 4 < a.coded_width &&
+              row * 4 < a.coded_height))
+            continue;
+        const bool vert = cc >= 1 && xp > 0;                              // pass 0 candidate
+        const bool horz = cr >= top && cr - top <= g.th / 4 && yp > 0;    // pass 1 candidate
+        if (!vert && !horz) continue;
         const uint8_t* map = side.tx[p ? 1 : 0];
         const int w = (((yp - py0) >> 2) + kWinTop) * kWinCols + ((xp - px0) >> 2) + kWinLeft;  // multiples of 4
         const int cur = map[w];
-        const int prev = PASS == 0 ? map[w - 1] : map[w - kWinCols];
-        const int cl = PASS == 0 ? tx_w_log2(cur) : tx_h_log2(cur);
-        const int pl = PASS == 0 ? tx_w_log2(prev) : tx_h_log2(prev);
-        if (((PASS == 0 ? xp : yp) & ((1 << cl) - 1)) != 0) continue;
-        const int size = min(p ? 8 : 16, 1 << min(cl, pl));
         const int r = row | g.sy, c = col | g.sx;
-        const int li = p == 0 ? PASS : p + 1;  // level index (7.14.5)
-        int lvl;
-        if (a.lvl_map) {
-            const int mi_r0 = y0 >> 2, mi_c0 = x0 >> 2;
-            const int lw = (r - mi_r0 + kWinTop) * kWinCols + c - mi_c0 + kWinLeft;
-            lvl = (side.lvl[lw] >> (8 * li)) & 0xFF;
-            if (lvl == 0) {
-                const int pw = PASS == 0 ? lw - (1 << g.sx) : lw - (kWinCols << g.sy);
-                lvl = (side.lvl[pw] >> (8 * li)) & 0xFF;
-            }
-        } else {
-            lvl = a.levels[li];
-        }
-        if (lvl == 0) continue;
-        const int cls = size == 4 ? 0 : p ? 1 : size == 8 ? 2 : 3;
+        const int lw = (r - mi_r0 + kWinTop) * kWinCols + c - mi_c0 + kWinLeft;
+        const uint32_t lv = a.lvl_map ? side.lvl[lw] : 0;
         const int off = (yp - py0 + kHalo) * g.pitch + (xp - px0 + kHalo);
-        const int nq = PASS == 0 ? P.width - xp : P.height - yp, np = PASS == 0 ? xp : yp;
-        const int at = atomicAdd(&s_count[cls], 1);
-        s_list[c_list_off[cls] + at] =
-            seg_entry(lvl, nq, np, off, p, PASS == 0 ? ia == 0 : ib == 0, PASS == 0 ? ia == na - 1 : ib == nb - 1);
+        if (vert) {
+            const int cl = tx_w_log2(cur), pl = tx_w_log2(map[w - 1]);
+            if ((xp & ((1 << cl) - 1)) == 0) {
+                const int li = p == 0 ? 0 : p + 1;  // level index (7.14.5)
+                int lvl;
+                if (a.lvl_map) {
+                    lvl = (lv >> (8 * li)) & 0xFF;
+                    if (lvl == 0) lvl = (side.lvl[lw - (1 << g.sx)] >> (8 * li)) & 0xFF;
+                } else {
+                    lvl = a.levels[li];
+                }
+                if (lvl != 0) {
+                    const int size = min(p ? 8 : 16, 1 << min(cl, pl));
+                    const int cls = size == 4 ? 0 : p ? 1 : size == 8 ? 2 : 3;
+                    const int at = atomicAdd(&s_count[cls], 1);
+                    s_list[c_list_off[cls] + at] = seg_entry(lvl, P.width - xp, xp, off, p, cr == 0, cr == nr - 1);
+                }
+            }
+        }
+        if (horz) {
+            const int cl = tx_h_log2(cur), pl = tx_h_log2(map[w - kWinCols]);
+            if ((yp & ((1 << cl) - 1)) == 0) {
+                const int li = p == 0 ? 1 : p + 1;
+                int lvl;
+                if (a.lvl_map) {
+                    lvl = (lv >> (8 * li)) & 0xFF;
+                    if (lvl == 0) lvl = (side.lvl[lw - (kWinCols << g.sy)] >> (8 * li)) & 0xFF;
+                } else {
+                    lvl = a.levels[li];
+                }
+                if (lvl != 0) {
+                    const int size = min(p ? 8 : 16, 1 << min(cl, pl));
+                    const int cls = size == 4 ? 0 : p ? 1 : size == 8 ? 2 : 3;
+                    const int at = atomicAdd(&s_count[4 + cls], 1);
+                    s_list[kListTotal + c_list_off[cls] + at] =
+                        seg_entry(lvl, P.height - yp, yp, off, p, cc == 0, cc == ncol - 1);
+                }
+            }
+        }
     }
 }
 
@@ -486,8 +511,7 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
 
     // ---- deblocking, pass 0 (vertical edges) then pass 1 (horizontal edges)
     if (a.deblock_on) {
-        deblock_lists<0, NT>(a, ssx, ssy, x0, y0, s_side, s_list, s_count);
-        deblock_lists<1, NT>(a, ssx, ssy, x0, y0, s_side, s_list + kListTotal, s_count + 4);
+        deblock_lists<NT>(a, ssx, ssy, x0, y0, s_side, s_list, s_count);
         __syncthreads();
         deblock_filter<0, NT>(a, ssx, ssy, smem, s_list, s_count, s_str);
         deblock_filter<1, NT>(a, ssx, ssy, smem, s_list + kListTotal, s_count + 4, s_str);
