@@ -437,6 +437,13 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
     }
 
     // ---- the launch sequence (captured once per composition when tuned so)
+    // the frames' common chroma layout (monochrome counts as 4:4:4), -1 if mixed
+    int layout = -2;
+    for (int i : order) {
+        const vaco_av1_frame_info& fi = jobs[i].info;
+        const int l = fi.monochrome ? 0 : fi.subsampling_x | fi.subsampling_y << 1;
+        layout = layout == -2 || layout == l ? l : -1;
+    }
     auto enqueue = [&]() -> cudaError_t {
         cudaError_t r = cudaMemcpyAsync(dtab, htab, table_bytes, cudaMemcpyHostToDevice, s);
         for (int i : order) {  // unfused: deblocking then CDEF, frame by frame
@@ -446,7 +453,7 @@ int32_t vaco::batch_enqueue(vaco_av1_ctx* ctx, cudaStream_t s, const vaco_av1_fr
         if (r == cudaSuccess && fused && !order.empty() && db_prefix[order.size()] > 0)
             r = launch_dbcdef_batch(dtab + off_db, reinterpret_cast<const int*>(dtab + off_db_prefix), (int)order.size(),
                                     db_prefix[order.size()], smem_db, ctx->tuning.dbcdef_ctas_per_sm,
-                                    ctx->tuning.dbcdef_threads, s);
+                                    ctx->tuning.dbcdef_threads, layout, s);
         for (int i : order) {
             const FramePlan& F = plan[i];
             if (r != cudaSuccess || !F.superres) continue;

@@ -683,15 +683,16 @@ __global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_kernel(DbCdefArgs a) {
 // hardware hands out the tiles in that order.  MIN_CTAS as for dbcdef_kernel.
 // (A persistent form, CTAs taking tiles from a device queue, kept its loop
 // state and the frame record live across the tile and spilled registers: it
-// measured 4 % slower on 4K frames.)
-template <int NT, int MIN_CTAS>
+// measured 4 % slower on 4K frames.)  LAYOUT as for dbcdef_tile: a batch
+// whose frames share one chroma layout takes the body compiled for it.
+template <int NT, int MIN_CTAS, int LAYOUT>
 __global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_batch_kernel(const DbCdefArgs* __restrict__ frames,
                                                                     const int* __restrict__ tile_prefix, int n) {
     const int f = frame_of_tile(tile_prefix, n, blockIdx.x);
     const DbCdefArgs& a = frames[f];
     const int local = blockIdx.x - tile_prefix[f];
     const int tiles_x = (a.mi_cols + 15) / 16;
-    dbcdef_tile<NT, -1>(a, local % tiles_x, local / tiles_x);
+    dbcdef_tile<NT, LAYOUT>(a, local % tiles_x, local / tiles_x);
 }
 
 }  // namespace
@@ -768,9 +769,9 @@ cudaError_t dbcdef_kernel_attributes() {
         for (auto k : {dbcdef_kernel<256, 4, 0>, dbcdef_kernel<256, 4, 1>, dbcdef_kernel<256, 4, 3>,
                        dbcdef_kernel<128, 5, 0>, dbcdef_kernel<128, 5, 1>, dbcdef_kernel<128, 5, 3>})
             if (e == cudaSuccess) e = cudaFuncSetAttribute(k, attr, kMaxSmem);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<256, 3>, attr, kMaxSmem);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<256, 4>, attr, kMaxSmem);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(dbcdef_batch_kernel<128, 5>, attr, kMaxSmem);
+        for (auto k : {dbcdef_batch_kernel<256, 3, -1>, dbcdef_batch_kernel<256, 3, 0>, dbcdef_batch_kernel<256, 3, 1>,
+                       dbcdef_batch_kernel<256, 3, 3>, dbcdef_batch_kernel<256, 4, -1>, dbcdef_batch_kernel<128, 5, -1>})
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k, attr, kMaxSmem);
         if (e != cudaSuccess) return e;
         g_attr_devices.fetch_or(1ull << dev, std::memory_order_release);
     }
@@ -794,17 +795,22 @@ cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
 }
 
 cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int n, int tiles, size_t smem,
-                                int ctas_per_sm, int threads, cudaStream_t stream) {
+                                int ctas_per_sm, int threads, int layout, cudaStream_t stream) {
     if (tiles <= 0) return cudaSuccess;
     cudaError_t e = dbcdef_kernel_attributes();
     if (e != cudaSuccess) return e;
     const DbCdefArgs* args = static_cast<const DbCdefArgs*>(dev_args);
-    if (threads == 128)
-        dbcdef_batch_kernel<128, 5><<<tiles, 128, smem, stream>>>(args, dev_prefix, n);
-    else if (ctas_per_sm <= 3)  // up to 3 resident: the 80-register body
-        dbcdef_batch_kernel<256, 3><<<tiles, 256, smem, stream>>>(args, dev_prefix, n);
-    else
-        dbcdef_batch_kernel<256, 4><<<tiles, 256, smem, stream>>>(args, dev_prefix, n);
+    using K = void (*)(const DbCdefArgs*, const int*, int);
+    K k;
+    if (threads == 128) {
+        k = dbcdef_batch_kernel<128, 5, -1>;
+    } else if (ctas_per_sm <= 3) {  // up to 3 resident: the 80-register body
+        k = layout == 3 ? dbcdef_batch_kernel<256, 3, 3> : layout == 1 ? dbcdef_batch_kernel<256, 3, 1>
+          : layout == 0 ? dbcdef_batch_kernel<256, 3, 0> : dbcdef_batch_kernel<256, 3, -1>;
+    } else {  // 64 registers: the layout-specialised bodies would spill
+        k = dbcdef_batch_kernel<256, 4, -1>;
+    }
+    k<<<tiles, threads == 128 ? 128 : 256, smem, stream>>>(args, dev_prefix, n);
     return cudaGetLastError();
 }
 

@@ -153,12 +153,14 @@ cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream);
 // bytes each, built by build_dbcdef_args), `dev_prefix` n+1 running tile
 // counts; one CTA per tile of all n frames (`tiles` = dev_prefix[n]).
 // `ctas_per_sm` (resident CTAs per SM the body is compiled for, i.e. its
-// register budget) and `threads` (per tile, 256 or 128) pick the kernel body.
+// register budget), `threads` (per tile, 256 or 128) and `layout` (the
+// frames' common chroma layout, ssx | ssy << 1 with monochrome as 0, or -1
+// when they differ) pick the kernel body.
 size_t dbcdef_args_size();
 size_t build_dbcdef_args(const DbCdefLaunch& L, void* out);  // returns dynamic smem bytes
 inline int dbcdef_tiles(const vaco_av1_frame_info& i) { return ((i.mi_cols + 15) / 16) * ((i.mi_rows + 15) / 16); }
 cudaError_t launch_dbcdef_batch(const void* dev_args, const int* dev_prefix, int n, int tiles, size_t smem,
-                                int ctas_per_sm, int threads, cudaStream_t stream);
+                                int ctas_per_sm, int threads, int layout, cudaStream_t stream);
 // Rows in the compact boundary buffer of a plane of `height` rows.
 inline int pre_rows_count(int height, int sub_y) {
     const int sh = 64 >> sub_y, off = 8 >> sub_y;
