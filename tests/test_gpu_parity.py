@@ -318,3 +318,25 @@ def test_upscale_picture_errors_follow_plane_order(ctx):
     cfg_eq = abi.SuperresPictureConfig(64, 64, 16, 1, 1, 0, 10)
     _, m = oracle.upscale_picture(planes, cfg_eq)
     _expect_same_error(lambda: ctx.upscale_picture(planes, cfg_eq), m)
+
+
+@pytest.mark.parametrize("bd", [8, 10, 12])
+def test_chain_extreme_samples(ctx, bd, oracle_threads):
+    """Planes of 4x4 cells drawn from {0, max, max/2, 1, max-1} with small
+    noise, at the highest loop-filter levels and every sharpness: the packed
+    deblocking arithmetic (biased narrow filter, 16-bit halves) meets its
+    extreme differences and saturating clamps."""
+    rng = np.random.default_rng(900 + bd)
+    maxv = (1 << bd) - 1
+    for seed, sharp in enumerate(range(8)):
+        f = synth.make_small(40 + seed, 200, 136, bd, sharpness=sharp, with_lvl_map=seed % 2 == 1)
+        f.deblock_levels = (63, 63, 63, 63) if seed % 3 else (40, 63, 12, 50)
+        for k, p in enumerate(f.planes):
+            cells = rng.choice(np.array([0, maxv, maxv // 2, 1, maxv - 1]), size=((p.shape[0] + 3) // 4,
+                                                                                  (p.shape[1] + 3) // 4))
+            v = np.repeat(np.repeat(cells, 4, 0), 4, 1)[: p.shape[0], : p.shape[1]].astype(np.int64)
+            v += rng.integers(-2, 3, size=v.shape)
+            f.planes[k] = np.clip(v, 0, maxv).astype(np.uint16)
+        want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+        assert m == 0
+        assert_planes_equal(ctx.postfilter_frame(f), want, f"extreme bd={bd} sharpness={sharp}")
