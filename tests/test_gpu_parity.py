@@ -340,3 +340,20 @@ def test_chain_extreme_samples(ctx, bd, oracle_threads):
         want, m = oracle.postfilter_frame(f, threads=oracle_threads)
         assert m == 0
         assert_planes_equal(ctx.postfilter_frame(f), want, f"extreme bd={bd} sharpness={sharp}")
+
+
+@pytest.mark.parametrize("lr_off", [(0,), (1, 2), (0, 1, 2)], ids=["y", "uv", "all"])
+@pytest.mark.parametrize("geom", [(200, 136, 10, None), (118, 70, 12, None), (60, 44, 8, None), (100, 58, 10, 124)])
+def test_chain_planes_without_restoration(ctx, lr_off, geom, oracle_threads):
+    """Planes whose restoration is off take the CDEF picture as their output
+    (without superres the fused kernel writes it there directly), next to
+    restored planes; odd visible widths end rows on a single sample."""
+    w, h, bd, up = geom
+    f = synth.make_small(60 + len(lr_off), w, h, bd, upscaled_width=up, sharpness=None, with_lvl_map=True)
+    f.lr_type = tuple(abi.FRAME_LR_NONE if k in lr_off else t for k, t in enumerate(f.lr_type))
+    want, m = oracle.postfilter_frame(f, threads=oracle_threads)
+    assert m == 0
+    assert_planes_equal(ctx.postfilter_frame(f), want, f"chain lr_off={lr_off}")
+    d = DeviceFrame(f)
+    ctx.postfilter_frame_dev(d)
+    assert_planes_equal(d.outputs_numpy(), want, f"chain dev lr_off={lr_off}")

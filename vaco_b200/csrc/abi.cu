@@ -873,6 +873,20 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
         if (!alloc_picture(ctx, &rows_like, np, S_PRE0, &pre_rows, &e)) return cuda_fail(ctx, e, msg);
         for (int k = 0; k < np; ++k) pre_rows_dp[k] = mplane(pre_rows, k);
     }
+    // Without superres, a plane whose restoration is off gets its output
+    // from the fused deblock+CDEF kernel itself (copy_visible_plane,
+    // decode.rs:673-681, with no copy afterwards), when the output is laid
+    // out for 32-bit stores.
+    DirectPlane direct[3] = {};
+    for (int k = 0; k < np && !superres; ++k) {
+        if (job->lr_type[k] != VACO_AV1_FRAME_LR_NONE) continue;
+        const int sx = k ? ssx : 0, sy = k ? ssy : 0;
+        const int w = info.upscaled_width >> sx, h = info.coded_height >> sy;
+        const DevPlane out{job->dst.planes[k], w, h, job->dst.stride[k]};
+        if (out.data && w > 0 && h > 0 && w <= job->dst.width[k] && h <= job->dst.height[k] &&
+            (out.stride & 1) == 0 && (reinterpret_cast<uintptr_t>(out.data) & 3) == 0)
+            direct[k] = DirectPlane{out};
+    }
     ctx->mark(0, s);
 
     // ---- deblocking + CDEF (host checks in the order deblock_frame / apply_cdef run them)
@@ -908,6 +922,7 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
             L.cdef = cp;
             L.status = ctx->status;
             L.threads = ctx->tuning.dbcdef_threads == 128 ? 128 : 256;
+            for (int k = 0; k < 3; ++k) L.direct[k] = direct[k];
             e = launch_dbcdef(L, s);
             ctx->launches++;
             if (e != cudaSuccess) return cuda_fail(ctx, e, msg);
@@ -973,8 +988,10 @@ static int32_t postfilter_dev_impl(vaco_av1_ctx* ctx, cudaStream_t s, const vaco
             if (job->lr_type[k] == VACO_AV1_FRAME_LR_NONE) {
                 // copy_visible_plane (decode.rs:673-681), as copy-only tiles
                 // of the same launch: SM copies run at HBM speed, a
-                // device-to-device memcpy at copy-engine speed.
-                lp[nlr++] = copy_only_plane(cplane(after, k), mplane(job->dst, k), w, h, (k && ssy) ? 1 : 0, k);
+                // device-to-device memcpy at copy-engine speed.  Nothing to
+                // do when the fused kernel wrote the plane (direct).
+                if (!direct[k].out.data)
+                    lp[nlr++] = copy_only_plane(cplane(after, k), mplane(job->dst, k), w, h, (k && ssy) ? 1 : 0, k);
                 continue;
             }
             if (job->lr_unit_size[k] == 0) {

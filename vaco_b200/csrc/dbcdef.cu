@@ -108,6 +108,7 @@ struct DbCdefArgs {
     DeviceStatus* status;
     int vec_ok;
     int staged_vectors;         // 16-byte vectors of all staged planes together
+    DirectPlane direct[3];      // final output written here too (see DirectPlane)
     size_t plane_off[3];        // shared-memory offset (samples) of each staged plane
 };
 
@@ -120,9 +121,10 @@ struct DbCdefArgs {
 // kShiftRows rows from row kHalo - 2 on the staged pitch, so every tap is a
 // single aligned word.
 template <int PITCH, int BH, int RPI, bool EDGE, bool SHIFT>
-__device__ __forceinline__ void filter_pairs(const uint16_t* t, const uint32_t* s1, const DevPlane& d, int px0,
-                                             int py0, int tw, const uint8_t* active, const PairBlock* blocks,
-                                             bool pri_on, bool sec_on, int br, int lane, int sx) {
+__device__ __forceinline__ void filter_pairs(const uint16_t* t, const uint32_t* s1, const DevPlane& d,
+                                             const DirectPlane* D, int px0, int py0, int tw, const uint8_t* active,
+                                             const PairBlock* blocks, bool pri_on, bool sec_on, int br, int lane,
+                                             int sx) {
     const int ppr = 32 / RPI;              // pairs per row
     const int lp = lane % ppr, lr = lane / ppr;
     const int x = 2 * lp;
@@ -138,6 +140,22 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const uint32_t* 
     uint32_t* o = reinterpret_cast<uint32_t*>(d.data + (long)(py0 + r0 + lr) * d.stride + gx);
     const long ostride = (long)d.stride * RPI / 2;  // words per RPI rows
     const uint32_t* cw = reinterpret_cast<const uint32_t*>(t + base_i);
+    // The final output too, for a plane without restoration (DirectPlane).
+    uint16_t* od = nullptr;
+    int od_rows = 0;
+    bool od_pair = false;
+    if (D && D->out.data && gx < D->out.width) {
+        od = D->out.data + (long)(py0 + r0 + lr) * D->out.stride + gx;
+        od_rows = min(BH, D->out.height - (py0 + r0));
+        od_pair = gx + 1 < D->out.width;
+    }
+    auto put = [&](int j, uint32_t v) {
+        if (od && lr + RPI * j < od_rows) {
+            uint16_t* q = od + (long)j * RPI * D->out.stride;
+            if (od_pair) *reinterpret_cast<uint32_t*>(q) = v;
+            else *q = (uint16_t)v;
+        }
+    };
     if ((pri_on || sec_on) && active[b]) {
         const PairBlock f = blocks[b];
         if (SHIFT) {
@@ -156,6 +174,7 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const uint32_t* 
                 const int woff = j * RPI * PITCH / 2;
                 const uint32_t v = filter_pair<EDGE>(cw[woff], taps, woff, f, pri_on, sec_on);
                 if (col_in && lr + RPI * j < rows_here) o[j * ostride] = v;
+                put(j, v);
             }
         } else {
             PairTap taps[12];
@@ -169,26 +188,31 @@ __device__ __forceinline__ void filter_pairs(const uint16_t* t, const uint32_t* 
                 const int woff = j * RPI * PITCH / 2;
                 const uint32_t v = filter_pair<EDGE>(cw[woff], taps, woff, f, pri_on, sec_on);
                 if (col_in && lr + RPI * j < rows_here) o[j * ostride] = v;
+                put(j, v);
             }
         }
     } else if (col_in) {
 #pragma unroll
-        for (int j = 0; j < BH / RPI; ++j)
-            if (lr + RPI * j < rows_here) o[j * ostride] = cw[j * RPI * PITCH / 2];
+        for (int j = 0; j < BH / RPI; ++j) {
+            const uint32_t v = cw[j * RPI * PITCH / 2];
+            if (lr + RPI * j < rows_here) o[j * ostride] = v;
+            put(j, v);
+        }
     }
 }
 
 template <int PITCH, int BH, int RPI, bool SHIFT>
 __device__ __forceinline__ void filter_pairs_edge(bool edge, const uint16_t* t, const uint32_t* s1, const DevPlane& d,
+                                                  const DirectPlane* D,
                                                   int px0, int py0, int tw, const uint8_t* active,
                                                   const PairBlock* blocks, bool pri_on, bool sec_on, int warp,
                                                   int lane, int sx, int nwarps) {
     for (int br = warp; br < 8; br += nwarps) {  // 8 block rows
         if (edge)
-            filter_pairs<PITCH, BH, RPI, true, SHIFT>(t, s1, d, px0, py0, tw, active, blocks, pri_on, sec_on, br, lane,
+            filter_pairs<PITCH, BH, RPI, true, SHIFT>(t, s1, d, D, px0, py0, tw, active, blocks, pri_on, sec_on, br, lane,
                                                      sx);
         else
-            filter_pairs<PITCH, BH, RPI, false, SHIFT>(t, s1, d, px0, py0, tw, active, blocks, pri_on, sec_on, br,
+            filter_pairs<PITCH, BH, RPI, false, SHIFT>(t, s1, d, D, px0, py0, tw, active, blocks, pri_on, sec_on, br,
                                                       lane, sx);
     }
 }
@@ -370,7 +394,7 @@ __device__ __forceinline__ void deblock_filter(const DbCdefArgs& a, int ssx, int
 // One 64x64 filter block (tile_x, tile_y) of one frame.  Every thread of the
 // CTA calls it; it ends with all threads past their last shared-memory use
 // only after the caller's next __syncthreads().
-template <int NT, int LAYOUT>
+template <int NT, int LAYOUT, bool DIRECT = false>
 __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int tile_y) {
     constexpr int kWarpsNT = NT / 32;
     // chroma subsampling: LAYOUT = ssx | ssy << 1 fixes it at compile time
@@ -549,12 +573,20 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
             const PlaneGeom g = plane_geom(p, ssx, ssy);
             const DevPlane& d = a.dst[p];
             const int px0 = x0 >> g.sx, py0 = y0 >> g.sy;
+            const DirectPlane* D = DIRECT ? &a.direct[p] : nullptr;
             const uint16_t* t = smem + a.plane_off[p];
             for (int r = warp; r < g.th; r += kWarpsNT) {
                 const int y = py0 + r;
                 if (y >= d.height) break;
-                for (int c = lane; c < g.tw; c += 32)
-                    if (px0 + c < d.width) d.data[(long)y * d.stride + px0 + c] = t[(r + kHalo) * g.pitch + c + kHalo];
+                for (int c = lane; c < g.tw; c += 32) {
+                    const int x = px0 + c;
+                    if (x >= d.width) continue;
+                    const uint16_t v = t[(r + kHalo) * g.pitch + c + kHalo];
+                    d.data[(long)y * d.stride + x] = v;
+                    // the final output too, for a plane without restoration
+                    if (D && D->out.data && y < D->out.height && x < D->out.width)
+                        D->out.data[(long)y * D->out.stride + x] = v;
+                }
             }
         }
         return;
@@ -651,16 +683,16 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
         }
         // tile layouts: 64x64 (luma, 4:4:4 chroma), 32x32 (4:2:0), 32x64 (4:2:2)
         if (p == 0) {
-            filter_pairs_edge<64 + 2 * kHalo, 8, 1, true>(edge, tp, s_u.shifted, d, px0, py0, g.tw, s_active,
+            filter_pairs_edge<64 + 2 * kHalo, 8, 1, true>(edge, tp, s_u.shifted, d, DIRECT ? &a.direct[p] : nullptr, px0, py0, g.tw, s_active,
                                                           s_pair[p], pri_on, sec_on, warp, lane, g.sx, kWarpsNT);
         } else if (g.tw == 64) {
-            filter_pairs_edge<64 + 2 * kHalo, 8, 1, false>(edge, tp, nullptr, d, px0, py0, g.tw, s_active, s_pair[p],
+            filter_pairs_edge<64 + 2 * kHalo, 8, 1, false>(edge, tp, nullptr, d, DIRECT ? &a.direct[p] : nullptr, px0, py0, g.tw, s_active, s_pair[p],
                                                            pri_on, sec_on, warp, lane, g.sx, kWarpsNT);
         } else if (g.th == 32) {
-            filter_pairs_edge<32 + 2 * kHalo, 4, 2, false>(edge, tp, nullptr, d, px0, py0, g.tw, s_active, s_pair[p],
+            filter_pairs_edge<32 + 2 * kHalo, 4, 2, false>(edge, tp, nullptr, d, DIRECT ? &a.direct[p] : nullptr, px0, py0, g.tw, s_active, s_pair[p],
                                                            pri_on, sec_on, warp, lane, g.sx, kWarpsNT);
         } else {
-            filter_pairs_edge<32 + 2 * kHalo, 8, 2, false>(edge, tp, nullptr, d, px0, py0, g.tw, s_active, s_pair[p],
+            filter_pairs_edge<32 + 2 * kHalo, 8, 2, false>(edge, tp, nullptr, d, DIRECT ? &a.direct[p] : nullptr, px0, py0, g.tw, s_active, s_pair[p],
                                                            pri_on, sec_on, warp, lane, g.sx, kWarpsNT);
         }
     }
@@ -672,10 +704,13 @@ __device__ __forceinline__ void dbcdef_tile(const DbCdefArgs& a, int tile_x, int
 // (1.5-2 % faster on the last two); 128 threads at 5 CTAs
 // per SM is the smaller-CTA shape (shorter barriers, about the same warps per
 // SM).  The batched form also has the 256 x 3 body (see dbcdef_batch_kernel).
-template <int NT, int MIN_CTAS, int LAYOUT>
+// DIRECT: a body that also writes the output of planes without restoration
+// (DirectPlane); the code for it measured 3 % slower on frames that have no
+// such plane, so it is a separate body.
+template <int NT, int MIN_CTAS, int LAYOUT, bool DIRECT = false>
 __global__ void __launch_bounds__(NT, MIN_CTAS) dbcdef_kernel(DbCdefArgs a) {
     overlap_prologue();
-    dbcdef_tile<NT, LAYOUT>(a, blockIdx.x, blockIdx.y);
+    dbcdef_tile<NT, LAYOUT, DIRECT>(a, blockIdx.x, blockIdx.y);
 }
 
 // Batched form: one CTA per tile of all frames of a batch, frames laid end to
@@ -751,6 +786,7 @@ size_t build_dbcdef_args(const DbCdefLaunch& L, void* out) {
     a.status = L.status;
     a.vec_ok = vec;
     a.staged_vectors = (int)(off / 8);  // each staged plane is a multiple of 8 samples
+    for (int p = 0; p < 3; ++p) a.direct[p] = p < np ? L.direct[p] : DirectPlane{};
     memcpy(out, &a, sizeof a);
     return off * sizeof(uint16_t);
 }
@@ -767,7 +803,9 @@ cudaError_t dbcdef_kernel_attributes() {
         const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
         cudaError_t e = cudaSuccess;
         for (auto k : {dbcdef_kernel<256, 4, 0>, dbcdef_kernel<256, 4, 1>, dbcdef_kernel<256, 4, 3>,
-                       dbcdef_kernel<128, 5, 0>, dbcdef_kernel<128, 5, 1>, dbcdef_kernel<128, 5, 3>})
+                       dbcdef_kernel<256, 4, 0, true>, dbcdef_kernel<256, 4, 1, true>,
+                       dbcdef_kernel<256, 4, 3, true>, dbcdef_kernel<128, 5, 0>, dbcdef_kernel<128, 5, 1>,
+                       dbcdef_kernel<128, 5, 3>})
             if (e == cudaSuccess) e = cudaFuncSetAttribute(k, attr, kMaxSmem);
         for (auto k : {dbcdef_batch_kernel<256, 3, -1>, dbcdef_batch_kernel<256, 3, 0>, dbcdef_batch_kernel<256, 3, 1>,
                        dbcdef_batch_kernel<256, 3, 3>, dbcdef_batch_kernel<256, 4, -1>, dbcdef_batch_kernel<128, 5, -1>})
@@ -784,8 +822,16 @@ cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream) {
     cudaError_t e = dbcdef_kernel_attributes();
     if (e != cudaSuccess) return e;
     dim3 grid(div_up(L.info.mi_cols, 16), div_up(L.info.mi_rows, 16));
-    // one kernel per chroma layout (4:4:4 and monochrome, 4:2:2, 4:2:0)
+    // one kernel per chroma layout (4:4:4 and monochrome, 4:2:2, 4:2:0); a
+    // frame with a plane written straight to the output takes the 256-thread
+    // body that does so, whatever the threads per tile
     const int layout = a.ssx | a.ssy << 1;
+    if (a.direct[0].out.data || a.direct[1].out.data || a.direct[2].out.data) {
+        auto k = layout == 3   ? dbcdef_kernel<256, 4, 3, true>
+                 : layout == 1 ? dbcdef_kernel<256, 4, 1, true>
+                               : dbcdef_kernel<256, 4, 0, true>;
+        return launch_overlapped(k, grid, dim3(256), smem, stream, a);
+    }
     if (L.threads == 128) {
         auto k = layout == 3 ? dbcdef_kernel<128, 5, 3> : layout == 1 ? dbcdef_kernel<128, 5, 1> : dbcdef_kernel<128, 5, 0>;
         return launch_overlapped(k, grid, dim3(128), smem, stream, a);

@@ -132,6 +132,13 @@ cudaError_t launch_deblock_prepare(const DevPlaneC* src, const DevPlane* dst, in
 cudaError_t launch_deblock_passes(const DeblockLaunch& L, cudaStream_t stream);
 
 // ---------------------------------------------------------------- fused deblock + CDEF
+// The final output of a plane without restoration in a frame without
+// superres, written by the fused deblock+CDEF kernel itself instead of
+// copied from the CDEF picture afterwards.
+struct DirectPlane {
+    DevPlane out;                    // visible output extent; data null: off
+};
+
 struct DbCdefLaunch {
     vaco_av1_picture src;       // reconstruction (device)
     vaco_av1_picture dst;       // CDEF output (device, same extents)
@@ -147,6 +154,7 @@ struct DbCdefLaunch {
     vaco_av1_cdef_params cdef;
     DeviceStatus* status;
     int threads = 256;          // threads per tile: 256 or 128
+    DirectPlane direct[3] = {};  // per plane; all off unless set
 };
 cudaError_t launch_dbcdef(const DbCdefLaunch& L, cudaStream_t stream);
 // Batched form: `dev_args` holds n per-frame argument records (dbcdef_args_size()
